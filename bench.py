@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the hst RK3 / Crank-Nicolson substep on B200s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2]
+
+One step is one RK3 time step (three substeps, hst_gpu_timestep, with the
+CFL read-back the Fortran time loop does every step); the metric is
+substeps per second of the whole job.  Default workload: BASELINE config 2,
+the plain FP64 drop-in at 384x384 dealiased x 256 (deck nx = 127, nz = 128,
+ny = 256; ly = 2 pi, alfa0 = beta0 = 1, S = 1, Re = 2000, dt = 0.002) from a
+seeded divergence-free field with E(k) ~ k^4 exp(-2 (k/8)^2), energy 0.1.
+The fields (0.4 GB per set of three components) are larger than L2, so no
+flush is needed between steps.
+
+N > 1 (one process per GPU under torch.distributed.run): independent
+replicas of the single-field path, which does not shard (the reference's
+pencil decomposition exists to spread one field over many GPUs; here one
+B200 holds it); no collective inside a step.  value = all ranks' substeps /
+the max over ranks of the device-timed region.
+
+--impl reference: the reference's CPU path on the host cores.  The
+reference (Fortran + MPI + FFTW) cannot be built in this image, so its
+restatement in oracle/ is timed instead (all host threads), rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PI = math.pi
+CONFIGS = {
+    # 96^2 x 64, Re 1000, dt 0.005, k0 4
+    "c1": dict(deck=dict(nx=31, ny=64, nz=32, alfa0=1.0, beta0=1.0, ly=2 * PI, re=1000.0, S=1.0, deltat=0.005),
+               k0=4.0, label="config 1: FP64 substep, 96x96 dealiased x 64 (nx=31, nz=32, ny=64), Re 1000, dt 0.005"),
+    # 384^2 x 256, Re 2000, dt 0.002, k0 8
+    "c2": dict(deck=dict(nx=127, ny=256, nz=128, alfa0=1.0, beta0=1.0, ly=2 * PI, re=2000.0, S=1.0, deltat=0.002),
+               k0=8.0, label="config 2: FP64 substep, 384x384 dealiased x 256 (nx=127, nz=128, ny=256), Re 2000, dt 0.002"),
+    # BASELINE config 3 geometry in FP64: 768^2 x 512, Re 5000, dt 0.001, exact_shift, k0 16
+    "c3": dict(deck=dict(nx=255, ny=512, nz=256, alfa0=1.0, beta0=1.0, ly=2 * PI, re=5000.0, S=1.0, deltat=0.001,
+                         exact_shift=True),
+               k0=16.0, label="config 3 geometry, FP64: 768x768 dealiased x 512 (nx=255, nz=256, ny=512), exact_shift"),
+}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def alg_bytes(deck, nxd, nzd):
+    """Compulsory HBM bytes per launch of each kernel and per substep (FP64).
+    Ns = ny (2nz+1)(nx+1) spectral points per component, Nzx = ny nzd (nx+1)."""
+    nx, ny, nz = deck["nx"], deck["ny"], deck["nz"]
+    Ns = ny * (2 * nz + 1) * (nx + 1)
+    Nzx = ny * nzd * (nx + 1)
+    b = 16.0
+    k = {
+        "zinv": b * (3 * Ns + 3 * Nzx),
+        "xprod": b * (3 * Nzx + 6 * Nzx),
+        "zfwd": b * (6 * Nzx + 6 * Ns),
+        "column": b * (16 * Ns),
+    }
+    return k, b * (25 * Ns + 18 * Nzx), Ns, Nzx
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def seeded_field(cfg, y):
+    from homogenenousshearturbulence_b200 import hst
+    d = cfg["deck"]
+    return hst.random_field(d["nx"], d["ny"], d["nz"], d["alfa0"], d["beta0"], d["ly"], y, seed=1, k0=cfg["k0"],
+                            energy=0.1)
+
+
+def cpu_oracle_rate(cfg, steps, budget_s=60.0):
+    """The oracle (the reference's CPU path restated, all host threads) on
+    the same workload; returns (substeps/s, steps timed, threads)."""
+    import oracle
+    from tests.gpu_util import deck_to_oracle
+    d = dict(cfg["deck"])
+    o = oracle.Sim(deck_to_oracle(d))
+    V0 = seeded_field(cfg, o.y())
+    for c in range(3):
+        o.field(c)[...] = V0[c]
+        o.fill_ghosts(c)
+    o.deltat = d["deltat"]
+    t0 = time.perf_counter()
+    o.timestep()  # warm-up step (page-in, plans)
+    first = time.perf_counter() - t0
+    n = max(1, min(steps, int(budget_s / max(first, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(n):
+        o.timestep()
+    el = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return 3 * n / el, n, threads
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    metric, unit = "substeps_per_s", "substeps/s"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        rate, n, threads = cpu_oracle_rate(cfg, args.steps, budget_s=90.0)
+        line = {"metric": metric, "value": rate, "unit": unit, "impl": "reference", "n_gpus": args.gpus,
+                "steps": n, "warmup": 1, "ms_per_step": 3000.0 / rate, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": cfg["label"], "step": "one RK3 time step = 3 substeps"},
+                "cpu_baseline": {"value": rate, "unit": unit, "cores": threads, "kind": "port",
+                                 "sample": f"{n} time steps of the same workload after 1 warm-up step (the oracle "
+                                           f"restatement of the reference CPU path; the Fortran+MPI+FFTW build is not "
+                                           f"buildable in this image)"},
+                "e2e": {"value": rate, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    from homogenenousshearturbulence_b200 import hst
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = local
+    torch.cuda.set_device(dev)
+    deck = dict(cfg["deck"])
+    dt = deck["deltat"]
+    s = hst.Solver(deck, device=dev)
+    V0 = seeded_field(cfg, s.y)
+    s.time = 0.0
+    s.set_velocity(V0)
+    stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", dev))
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        s.sync()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        s.timestep(dt)
+    barrier()
+    launches0 = s.launches
+    s.reset_kernel_times()
+    s.set_profiling(True)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.timestep(dt)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    s.set_profiling(False)
+    ktimes = s.kernel_times()
+    launches = s.launches - launches0
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    nsub = 3 * args.steps
+    value = world * nsub / (ms / 1000.0)
+    if not math.isfinite(s.cfl):
+        raise SystemExit("non-finite CFL: the run blew up")
+
+    # end to end through the public API with host buffers: every step
+    # uploads the three velocity components from pinned memory, advances
+    # one time step and downloads them again
+    e2e = None
+    if not args.no_e2e:
+        nbytes = s.shape[0] * s.shape[1] * s.shape[2] * 16
+        pin = [torch.empty(nbytes, dtype=torch.uint8, pin_memory=True) for _ in range(3)]
+        for c in range(3):
+            s.download_ptr(c, pin[c].data_ptr())
+        ke = max(3, args.steps // 2)
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(ke):
+            for c in range(3):
+                s.upload_ptr(c, pin[c].data_ptr())
+            s.timestep(dt)
+            for c in range(3):
+                s.download_ptr(c, pin[c].data_ptr())
+        f1.record(stream)
+        f1.synchronize()
+        mse = f0.elapsed_time(f1)
+        if dist is not None:
+            t = torch.tensor([mse], device=f"cuda:{dev}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            mse = float(t.item())
+        e2e = {"value": world * 3 * ke / (mse / 1000.0), "unit": unit, "h2d_bytes_per_step": 3 * nbytes,
+               "d2h_bytes_per_step": 3 * nbytes + 8, "steps": ke}
+
+    if rank == 0:
+        per_kernel, b_sub, Ns, Nzx = alg_bytes(deck, s.nxd, s.nzd)
+        peak, peak_kind = peaks()
+        kt = {k: v for k, v in ktimes.items() if v[1] > 0}
+        top = max(kt, key=lambda k: kt[k][0])
+        avg_ms = kt[top][0] / kt[top][1]
+        achieved = per_kernel[top] / (avg_ms / 1000.0) / 1e9
+        traffic = None
+        tf = ROOT / "profiles" / f"traffic_{args.config}.json"
+        if tf.exists():
+            traffic = json.loads(tf.read_text()).get(top)
+        sub_ms = ms / nsub
+        line = {
+            "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["label"], "step": "one RK3 time step = 3 substeps (hst_gpu_timestep)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single field, 1 GPU",
+                       "l2": "inputs larger than L2 (no flush)", "nxd": s.nxd, "nzd": s.nzd,
+                       },
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "alg_bytes_per_launch": per_kernel[top], "avg_launch_ms": avg_ms},
+            "substep_roofline": {"alg_bytes": b_sub, "ms_per_substep": sub_ms,
+                                 "achieved_gbs": b_sub / (sub_ms / 1000.0) / 1e9,
+                                 "frac": b_sub / (sub_ms / 1000.0) / 1e9 / peak},
+            "kernels_ms_per_launch": {k: v[0] / v[1] for k, v in kt.items()},
+            "kernel_share": {k: v[0] / sum(x[0] for x in kt.values()) for k, v in kt.items()},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if world == 1 and not args.no_cpu_baseline:
+            rate, n, threads = cpu_oracle_rate(cfg, 2, budget_s=20.0)
+            line["cpu_baseline"] = {"value": rate, "unit": unit, "cores": threads, "kind": "port",
+                                    "sample": f"{n} time step(s) of the same workload after 1 warm-up step, oracle "
+                                              f"restatement of the reference CPU path, {threads} threads"}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,678 @@
+// The C ABI of include/hst_gpu.h: the context, its tables and the host-side
+// sequencing of the substep.  Host arithmetic that feeds the device (grid,
+// der, damping table, wrap displacements, S2 law, time) follows the
+// reference's host code in the same operation order, so that a Fortran
+// driver that passes its own tables and one that lets the context build them
+// get the same numbers.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "hst_internal.h"
+
+using hst::DeviceState;
+using hst::Geometry;
+using hst::PhysScalars;
+using hst::SubstepScalars;
+
+namespace {
+const double PI = 3.141592653589793;
+const double TWOPI = 6.283185307179586;
+
+// x**n for a variable integer n, as gfortran evaluates it (binary powering)
+double powi(double x, int m) {
+  unsigned n = m < 0 ? -m : m;
+  double y = (n % 2) ? x : 1.0;
+  while (n >>= 1) {
+    x = x * x;
+    if (n % 2) y = y * x;
+  }
+  return m < 0 ? 1.0 / y : y;
+}
+double fmodulo(double a, double p) {
+  double r = std::fmod(a, p);
+  if (r != 0.0 && ((r < 0.0) != (p < 0.0))) r += p;
+  return r;
+}
+int imodulo(int a, int p) {
+  int r = a % p;
+  if (r != 0 && ((r < 0) != (p < 0))) r += p;
+  return r;
+}
+bool fft_fit(int n) {  // src/hst_input.f90:107-115
+  if (n <= 0) return false;
+  int j = n;
+  while (j % 2 == 0) j /= 2;
+  return j == 1 || j == 3;
+}
+double ymap(double xi, double ystretch) {  // src/hst_setup.f90:80-89
+  if (ystretch <= 1.0e-10) return xi;
+  if (xi <= 0.5) return 0.5 * std::tanh(2.0 * ystretch * xi) / std::tanh(ystretch);
+  return 0.5 * (2.0 + std::tanh(2.0 * ystretch * (xi - 1.0)) / std::tanh(ystretch));
+}
+// dense 5x5 solve with partial pivoting (src/hst_derivatives.f90:59-79)
+void solve5(const double Min[5][5], const double bin[5], double x[5]) {
+  double M[5][5], b[5];
+  std::memcpy(M, Min, sizeof M);
+  std::memcpy(b, bin, sizeof b);
+  for (int i = 0; i <= 4; ++i) {
+    int p = i;
+    double best = std::fabs(M[i][i]);
+    for (int r = i + 1; r <= 4; ++r)
+      if (std::fabs(M[r][i]) > best) {
+        best = std::fabs(M[r][i]);
+        p = r;
+      }
+    if (p != i) {
+      for (int c = 0; c <= 4; ++c) std::swap(M[i][c], M[p][c]);
+      std::swap(b[i], b[p]);
+    }
+    for (int j = i + 1; j <= 4; ++j) {
+      double f = M[j][i] / M[i][i];
+      for (int c = i; c <= 4; ++c) M[j][c] = M[j][c] - f * M[i][c];
+      b[j] = b[j] - f * b[i];
+    }
+  }
+  for (int i = 4; i >= 0; --i) {
+    double s = 0.0;
+    for (int c = i + 1; c <= 4; ++c) s = s + M[i][c] * x[c];
+    x[i] = (b[i] - s) / M[i][i];
+  }
+}
+// setup_derivatives (src/hst_derivatives.f90:30-56); y has the ghost rows
+void setup_derivatives(int ny, const std::vector<double>& y, std::vector<double>& der) {
+  der.assign((size_t)ny * 20, 0.0);
+  for (int iy = 0; iy < ny; ++iy) {
+    double dyj[5];
+    for (int j = -2; j <= 2; ++j) dyj[j + 2] = y[iy + j + 2] - y[iy + 2];
+    double M[5][5], t[5], d4[5], d0[5], d2[5], d1[5];
+    for (int i = 0; i <= 4; ++i)
+      for (int j = 0; j <= 4; ++j) M[i][j] = powi(dyj[j], 4 - i);
+    for (int i = 0; i < 5; ++i) t[i] = 0.0;
+    t[0] = 24.0;
+    solve5(M, t, d4);
+    for (int i = 0; i <= 4; ++i)
+      for (int j = 0; j <= 4; ++j) M[i][j] = (double)((5 - i) * (6 - i) * (7 - i) * (8 - i)) * powi(dyj[j], 4 - i);
+    for (int i = 0; i <= 4; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < 5; ++j) s = s + d4[j] * powi(dyj[j], 8 - i);
+      t[i] = s;
+    }
+    solve5(M, t, d0);
+    for (int i = 0; i <= 4; ++i)
+      for (int j = 0; j <= 4; ++j) M[i][j] = powi(dyj[j], 4 - i);
+    for (int i = 0; i < 5; ++i) t[i] = 0.0;
+    for (int i = 0; i <= 2; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < 5; ++j) s = s + d0[j] * (double)(4 - i) * (double)(3 - i) * powi(dyj[j], 2 - i);
+      t[i] = s;
+    }
+    solve5(M, t, d2);
+    for (int i = 0; i < 5; ++i) t[i] = 0.0;
+    for (int i = 0; i <= 3; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < 5; ++j) s = s + d0[j] * (double)(4 - i) * powi(dyj[j], 3 - i);
+      t[i] = s;
+    }
+    solve5(M, t, d1);
+    const double* rows[4] = {d0, d1, d2, d4};
+    for (int n = 0; n < 4; ++n)
+      for (int j = 0; j < 5; ++j) der[(size_t)iy + (size_t)ny * (n + 4 * j)] = rows[n][j];
+  }
+}
+}  // namespace
+
+struct hst_ctx {
+  hst_gpu_params p;
+  Geometry g;
+  DeviceState d;
+  PhysScalars ps;
+  double lx, lz;
+  std::vector<double> y, dyl, der, gdamp;
+  double theta_last;
+  cudaStream_t stream;
+  double* h_gdamp;                // pinned staging of gdamp uploads
+  unsigned long long* h_cfl;      // pinned CFL read-back
+  std::string err;
+  long long launches;
+  int device;
+  // per-kernel-class CUDA-event accounting (hst_gpu_set_profiling)
+  bool prof_on;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> ev_class;  // class of each recorded pair
+  double prof_ms[HST_KC_N];
+  long long prof_n[HST_KC_N];
+};
+
+// Runs `launch` (which queues one kernel on ctx->stream) between two events
+// when profiling is on, and counts it.
+template <typename F>
+static cudaError_t timed(hst_ctx* c, int kc, F launch) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (c->prof_on) {
+    size_t k = c->ev_class.size();
+    while (c->ev.size() < 2 * (k + 1)) {
+      cudaEvent_t e;
+      cudaError_t r = cudaEventCreate(&e);
+      if (r != cudaSuccess) return r;
+      c->ev.push_back(e);
+    }
+    a = c->ev[2 * k];
+    b = c->ev[2 * k + 1];
+    cudaEventRecord(a, c->stream);
+  }
+  cudaError_t r = launch();
+  if (r != cudaSuccess) return r;
+  c->launches++;
+  if (c->prof_on) {
+    cudaEventRecord(b, c->stream);
+    c->ev_class.push_back(kc);
+  }
+  return cudaSuccess;
+}
+
+static int fail(hst_ctx* c, int code, const char* fmt, ...) {
+  if (c) {
+    char b[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(b, sizeof b, fmt, ap);
+    va_end(ap);
+    c->err = b;
+  }
+  return code;
+}
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return fail(ctx, HST_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+// ------------------------------------------------------ host scalars ----
+static double s2_of(const hst_gpu_params& p, double t) {  // src/hst_derivatives.f90:85-95
+  if ((p.s2_amplitude == 0.0 && p.s2_mean == 0.0) || t < p.s2_start) return 0.0;
+  if (p.s2_period > 0.0) return p.s2_mean + p.s2_amplitude * std::sin(TWOPI / p.s2_period * (t - p.s2_start));
+  return p.s2_mean + p.s2_amplitude;
+}
+static double s2_integral(const hst_gpu_params& p, double t1, double t2) {  // :98-112
+  if ((p.s2_amplitude == 0.0 && p.s2_mean == 0.0) || t2 <= p.s2_start) return 0.0;
+  double a = std::max(t1, p.s2_start), b = t2;
+  if (p.s2_period > 0.0) {
+    double omega = TWOPI / p.s2_period;
+    return p.s2_mean * (b - a) + p.s2_amplitude / omega * (std::cos(omega * (a - p.s2_start)) - std::cos(omega * (b - p.s2_start)));
+  }
+  return (p.s2_mean + p.s2_amplitude) * (b - a);
+}
+static void shear_shifts(const hst_ctx* c, double t, double* sx, double* sz) {  // :123-128
+  *sx = fmodulo(c->p.S * t * c->p.ly, c->lx);
+  *sz = fmodulo(s2_integral(c->p, c->p.s2_start, t) * c->p.ly, c->lz);
+}
+static bool damping_active(const hst_gpu_params& p) {  // src/hst_damping.f90:46-48
+  return p.damp_kpar > 0.0 && p.damp_kperp > 0.0 && (p.damp_hard || p.damp_rate > 0.0);
+}
+// damping_update (src/hst_damping.f90:80-115); true when the table changed
+static bool damping_update(hst_ctx* c, double t) {
+  const hst_gpu_params& p = c->p;
+  double theta = p.damp_follow ? std::atan2(s2_of(p, t), p.S) : p.damp_angle * PI / 180.0;
+  if (theta == c->theta_last) return false;
+  c->theta_last = theta;
+  double cs = std::cos(theta), sn = std::sin(theta);
+  for (int ix = 0; ix <= p.nx; ++ix) {
+    double kx = p.alfa0 * ix;
+    for (int iz = -p.nz; iz <= p.nz; ++iz) {
+      double kz = p.beta0 * iz;
+      double kpar = kx * cs + kz * sn, kperp = -kx * sn + kz * cs;
+      double r = std::pow(std::pow(std::fabs(kpar) / p.damp_kpar, p.damp_norm) + std::pow(std::fabs(kperp) / p.damp_kperp, p.damp_norm),
+                          1.0 / p.damp_norm);
+      double g = 0.0;
+      if (r < 1.0 - 1.0e-6) {
+        if (p.damp_hard) g = 1.0;
+        else if (r <= 1.0 - p.damp_edge) g = p.damp_rate;
+        else {
+          double x = (1.0 - r) / p.damp_edge;
+          g = p.damp_rate * x * x * (3.0 - 2.0 * x);
+        }
+      }
+      if (ix == 0 && iz == 0 && !p.damp_mean) g = 0.0;
+      c->gdamp[(size_t)(iz + p.nz) + (size_t)(2 * p.nz + 1) * ix] = g;
+    }
+  }
+  return true;
+}
+
+// ------------------------------------------------------ geometry ----
+static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& why) {
+  g.nx = p.nx;
+  g.ny = p.ny;
+  g.nz = p.nz;
+  g.nxd = p.nxd;
+  g.nzd = p.nzd;
+  if (g.nxd <= 0) {
+    g.nxd = 3 * (p.nx + 1) / 2;
+    while (!fft_fit(g.nxd)) g.nxd++;
+  }
+  if (g.nzd <= 0) {
+    g.nzd = 3 * p.nz;
+    while (!fft_fit(g.nzd)) g.nzd++;
+  }
+  if (p.nx < 1 || p.nz < 1 || p.ny < 8) {
+    why = "need nx >= 1, nz >= 1, ny >= 8";
+    return HST_EARG;
+  }
+  if (!fft_fit(g.nxd) || !fft_fit(g.nzd) || 2 * g.nxd < 3 * (p.nx + 1) - 1 || g.nzd < 3 * p.nz) {
+    why = "nxd, nzd must be 2^a 3^b (b <= 1) and satisfy the 3/2 rule";
+    return HST_EARG;
+  }
+  if (p.ny % 2 != 0) {
+    why = "ny must be even";
+    return HST_EARG;
+  }
+  g.nxB = p.nx + 1;
+  g.nzT = 2 * p.nz + 1;
+  g.rows = p.ny + 4;
+  g.ncol = g.nxB * g.nzT;
+  g.nf = (long)g.ncol * g.rows;
+  // line-solve group: P lanes of m rows; prefer m >= 16, accept m >= 4
+  int P = 0;
+  const char* env = std::getenv("HST_LINE_LANES");
+  if (env) {
+    int e = std::atoi(env);
+    if (e >= 2 && e <= 32 && (e & (e - 1)) == 0 && p.ny % e == 0 && p.ny / e >= 4) P = e;
+  }
+  for (int mmin : {16, 8, 4}) {
+    if (P) break;
+    for (int c = 32; c >= 2; c >>= 1)
+      if (p.ny % c == 0 && p.ny / c >= mmin) {
+        P = c;
+        break;
+      }
+  }
+  if (!P) {
+    why = "ny must be a multiple of 2 with at least 4 rows per lane";
+    return HST_EARG;
+  }
+  g.P = P;
+  g.m = p.ny / P;
+  g.MS = g.m | 1;
+  // transform y tile
+  g.Ty = 2;
+  for (int t : {8, 4}) {
+    if (p.ny % t == 0 && (size_t)t * (g.nzd + 1) * 16 <= 100 * 1024) {
+      g.Ty = t;
+      break;
+    }
+  }
+  g.ppt = 8;
+  if (2 * g.nxd * 6 / 8 > 1024 || g.Ty * g.nzd / 8 > 1024) {
+    why = "transform length too large for this build";
+    return HST_EARG;
+  }
+  return HST_OK;
+}
+
+static double dev_bytes(const Geometry& g) {
+  double nf = (double)g.nf;
+  double z = 3.0 * g.nzd * g.ny * g.nxB, pp = 6.0 * g.nzd * g.ny * g.nxB, q = 6.0 * g.ncol * g.ny;
+  return 16.0 * (7.0 * nf + z + pp + q) + 8.0 * (20.0 * g.ny + 2.0 * g.ny + 4 + g.ncol);
+}
+
+extern "C" double hst_gpu_device_bytes(const hst_gpu_params* p) {
+  Geometry g;
+  std::string why;
+  if (!p || choose_geometry(*p, g, why) != HST_OK) return 0.0;
+  return dev_bytes(g);
+}
+
+static std::vector<double2> twiddles(int n) {
+  std::vector<double2> t(n);
+  for (int k = 0; k < n; ++k) {
+    long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)n;
+    t[k] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  return t;
+}
+
+static void free_device(hst_ctx* c) {
+  DeviceState& d = c->d;
+  for (int i = 0; i < 7; ++i)
+    if (d.F[i]) cudaFree(d.F[i]);
+  void* ps[] = {d.Z, d.Pp, d.Q, d.der, d.y, d.dyl, d.gdamp, d.twx, d.twz, d.cfl};
+  for (void* q : ps)
+    if (q) cudaFree(q);
+  std::memset(&d, 0, sizeof d);
+}
+
+extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
+  if (!pin || !out) return HST_EARG;
+  *out = nullptr;
+  hst_ctx* ctx = new (std::nothrow) hst_ctx();
+  if (!ctx) return HST_ENOMEM;
+  ctx->p = *pin;
+  ctx->launches = 0;
+  ctx->prof_on = false;
+  for (int k = 0; k < HST_KC_N; ++k) {
+    ctx->prof_ms[k] = 0.0;
+    ctx->prof_n[k] = 0;
+  }
+  ctx->stream = nullptr;
+  ctx->h_gdamp = nullptr;
+  ctx->h_cfl = nullptr;
+  std::memset(&ctx->d, 0, sizeof ctx->d);
+  std::string why;
+  int rc = choose_geometry(*pin, ctx->g, why);
+  if (rc != HST_OK) {
+    std::fprintf(stderr, "hst_gpu_create: %s\n", why.c_str());
+    delete ctx;
+    return rc;
+  }
+  ctx->p.nxd = ctx->g.nxd;
+  ctx->p.nzd = ctx->g.nzd;
+  const hst_gpu_params& p = ctx->p;
+  const Geometry& g = ctx->g;
+  ctx->device = p.device;
+  // derived quantities (src/hst_input.f90:206-215)
+  ctx->lx = 2.0 * PI / p.alfa0;
+  ctx->lz = 2.0 * PI / p.beta0;
+  ctx->ps.alfa0 = p.alfa0;
+  ctx->ps.beta0 = p.beta0;
+  ctx->ps.ni = 1.0 / p.re;
+  ctx->ps.S = p.S;
+  ctx->ps.dx = PI / (p.alfa0 * g.nxd);
+  ctx->ps.dz = 2.0 * PI / (p.beta0 * g.nzd);
+  ctx->ps.factor = 1.0 / (2.0 * g.nxd * g.nzd);
+  // grid (src/hst_setup.f90:42-71)
+  const int ny = p.ny;
+  ctx->y.resize(ny + 4);
+  for (int iy = -2; iy <= ny + 1; ++iy) {
+    int mo = imodulo(iy, ny);
+    ctx->y[iy + 2] = p.ly * ymap((double)mo / ny, p.ystretch) + p.ly * (double)((iy - mo) / ny);
+  }
+  ctx->dyl.resize(ny);
+  for (int iy = 0; iy < ny; ++iy) ctx->dyl[iy] = 0.5 * (ctx->y[iy + 3] - ctx->y[iy + 1]);
+  setup_derivatives(ny, ctx->y, ctx->der);
+  ctx->gdamp.assign((size_t)g.ncol, 0.0);
+  ctx->theta_last = -1.0e308;
+  if (damping_active(p)) damping_update(ctx, 0.0);
+
+  if (cudaSetDevice(p.device) != cudaSuccess) {
+    std::fprintf(stderr, "hst_gpu_create: cannot select CUDA device %d\n", p.device);
+    delete ctx;
+    return HST_ECUDA;
+  }
+  auto alloc = [&](void** ptr, size_t bytes) -> bool {
+    if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return true;
+  };
+  DeviceState& d = ctx->d;
+  bool ok = true;
+  for (int i = 0; i < 7 && ok; ++i) ok = alloc((void**)&d.F[i], sizeof(double2) * g.nf);
+  ok = ok && alloc((void**)&d.Z, sizeof(double2) * 3 * (size_t)g.nzd * g.ny * g.nxB);
+  ok = ok && alloc((void**)&d.Pp, sizeof(double2) * 6 * (size_t)g.nzd * g.ny * g.nxB);
+  ok = ok && alloc((void**)&d.Q, sizeof(double2) * 6 * (size_t)g.ncol * g.ny);
+  ok = ok && alloc((void**)&d.der, sizeof(double) * 20 * (size_t)ny);
+  ok = ok && alloc((void**)&d.y, sizeof(double) * (ny + 4));
+  ok = ok && alloc((void**)&d.dyl, sizeof(double) * ny);
+  ok = ok && alloc((void**)&d.gdamp, sizeof(double) * g.ncol);
+  ok = ok && alloc((void**)&d.twx, sizeof(double2) * 2 * g.nxd);
+  ok = ok && alloc((void**)&d.twz, sizeof(double2) * g.nzd);
+  ok = ok && alloc((void**)&d.cfl, sizeof(unsigned long long));
+  if (!ok) {
+    free_device(ctx);
+    std::fprintf(stderr, "hst_gpu_create: device allocation of %.2f GB refused\n", dev_bytes(g) / 1e9);
+    delete ctx;
+    return HST_ENOMEM;
+  }
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMallocHost((void**)&ctx->h_gdamp, sizeof(double) * g.ncol) != cudaSuccess ||
+      cudaMallocHost((void**)&ctx->h_cfl, sizeof(unsigned long long)) != cudaSuccess) {
+    free_device(ctx);
+    delete ctx;
+    return HST_ECUDA;
+  }
+  for (int i = 0; i < 7; ++i) cudaMemsetAsync(d.F[i], 0, sizeof(double2) * g.nf, ctx->stream);
+  auto tx = twiddles(2 * g.nxd), tz = twiddles(g.nzd);
+  cudaMemcpy(d.der, ctx->der.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice);
+  cudaMemcpy(d.y, ctx->y.data(), sizeof(double) * (ny + 4), cudaMemcpyHostToDevice);
+  cudaMemcpy(d.dyl, ctx->dyl.data(), sizeof(double) * ny, cudaMemcpyHostToDevice);
+  cudaMemcpy(d.gdamp, ctx->gdamp.data(), sizeof(double) * g.ncol, cudaMemcpyHostToDevice);
+  cudaMemcpy(d.twx, tx.data(), sizeof(double2) * tx.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(d.twz, tz.data(), sizeof(double2) * tz.size(), cudaMemcpyHostToDevice);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "hst_gpu_create: %s\n", cudaGetErrorString(e));
+    free_device(ctx);
+    delete ctx;
+    return HST_ECUDA;
+  }
+  *out = ctx;
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_destroy(hst_ctx* ctx) {
+  if (!ctx) return HST_EARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
+  free_device(ctx);
+  if (ctx->h_gdamp) cudaFreeHost(ctx->h_gdamp);
+  if (ctx->h_cfl) cudaFreeHost(ctx->h_cfl);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return HST_OK;
+}
+
+extern "C" const char* hst_gpu_last_error(const hst_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+extern "C" long long hst_gpu_launch_count(const hst_ctx* ctx) { return ctx ? ctx->launches : 0; }
+extern "C" void* hst_gpu_stream(const hst_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+extern "C" int hst_gpu_set_tables(hst_ctx* ctx, const double* der, const double* y, const double* dyl) {
+  if (!ctx) return HST_EARG;
+  const int ny = ctx->p.ny;
+  CK(cudaSetDevice(ctx->device));
+  if (der) {
+    std::memcpy(ctx->der.data(), der, sizeof(double) * 20 * ny);
+    CK(cudaMemcpyAsync(ctx->d.der, ctx->der.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (y) {
+    std::memcpy(ctx->y.data(), y, sizeof(double) * (ny + 4));
+    CK(cudaMemcpyAsync(ctx->d.y, ctx->y.data(), sizeof(double) * (ny + 4), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (dyl) {
+    std::memcpy(ctx->dyl.data(), dyl, sizeof(double) * ny);
+    CK(cudaMemcpyAsync(ctx->d.dyl, ctx->dyl.data(), sizeof(double) * ny, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_get_tables(const hst_ctx* c, double* der, double* y, double* dyl) {
+  if (!c) return HST_EARG;
+  const int ny = c->p.ny;
+  if (der) std::memcpy(der, c->der.data(), sizeof(double) * 20 * ny);
+  if (y) std::memcpy(y, c->y.data(), sizeof(double) * (ny + 4));
+  if (dyl) std::memcpy(dyl, c->dyl.data(), sizeof(double) * ny);
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_upload(hst_ctx* ctx, int field, const double* host) {
+  if (!ctx || field < 0 || field > 6 || !host) return fail(ctx, HST_EARG, "upload: bad field %d", field);
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(ctx->d.F[field], host, sizeof(double2) * ctx->g.nf, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_download(hst_ctx* ctx, int field, double* host) {
+  if (!ctx || field < 0 || field > 6 || !host) return fail(ctx, HST_EARG, "download: bad field %d", field);
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(host, ctx->d.F[field], sizeof(double2) * ctx->g.nf, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_sync(hst_ctx* ctx) {
+  if (!ctx) return HST_EARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_shear_shifts(const hst_ctx* c, double t, double* sx, double* sz) {
+  if (!c || !sx || !sz) return HST_EARG;
+  shear_shifts(c, t, sx, sz);
+  return HST_OK;
+}
+extern "C" double hst_gpu_s2_of(const hst_ctx* c, double t) { return c ? s2_of(c->p, t) : 0.0; }
+extern "C" double hst_gpu_s2_integral(const hst_ctx* c, double t1, double t2) {
+  return c ? s2_integral(c->p, t1, t2) : 0.0;
+}
+
+extern "C" int hst_gpu_fill_ghosts(hst_ctx* ctx, int field, double sx, double sz) {
+  if (!ctx || field < 0 || field > 6) return fail(ctx, HST_EARG, "fill_ghosts: bad field %d", field);
+  CK(cudaSetDevice(ctx->device));
+  CK(timed(ctx, HST_KC_GHOSTS, [&] { return hst::launch_fill_ghosts(ctx->g, ctx->d, ctx->ps, field, sx, sz, ctx->stream); }));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_fill_ghosts_at(hst_ctx* ctx, int field, double time) {
+  if (!ctx) return HST_EARG;
+  double sx, sz;
+  shear_shifts(ctx, time, &sx, &sz);
+  return hst_gpu_fill_ghosts(ctx, field, sx, sz);
+}
+
+extern "C" int hst_gpu_line_solve(hst_ctx* ctx, int sys, double lambda, int src, int dst, int has_shift, double sx,
+                                  double sz, double time) {
+  if (!ctx || sys < 1 || sys > 5 || src < 0 || src > 6 || dst < 0 || dst > 6 || src == dst)
+    return fail(ctx, HST_EARG, "line_solve: bad arguments (sys %d, src %d, dst %d)", sys, src, dst);
+  if (!has_shift) shear_shifts(ctx, time, &sx, &sz);
+  CK(cudaSetDevice(ctx->device));
+  CK(timed(ctx, HST_KC_LINE_SOLVE,
+           [&] { return hst::launch_line_solve(ctx->g, ctx->d, ctx->ps, sys, lambda, src, dst, sx, sz, ctx->stream); }));
+  return HST_OK;
+}
+
+static int read_cfl(hst_ctx* ctx, double* cfl) {
+  CK(cudaMemcpyAsync(ctx->h_cfl, ctx->d.cfl, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  unsigned long long b = *ctx->h_cfl;
+  double v;
+  std::memcpy(&v, &b, sizeof v);
+  if (cfl) *cfl = v;
+  if (!std::isfinite(v)) return fail(ctx, HST_EFINITE, "non-finite CFL number %g", v);
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_compute_cfl(hst_ctx* ctx, double* cfl) {
+  if (!ctx) return HST_EARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemsetAsync(ctx->d.cfl, 0, sizeof(unsigned long long), ctx->stream));
+  CK(timed(ctx, HST_KC_ZINV, [&] { return hst::launch_zinv(ctx->g, ctx->d, ctx->stream); }));
+  CK(timed(ctx, HST_KC_XPROD, [&] { return hst::launch_xprod(ctx->g, ctx->d, ctx->ps, 1, ctx->stream); }));
+  return read_cfl(ctx, cfl);
+}
+
+// One time step (src/hst_equations.f90:56-87) queued on the stream.
+static int queue_timestep(hst_ctx* ctx, double* time, double deltat) {
+  static const double RK[3][3] = {{120.0 / 32.0, 2.0, 0.0}, {120.0 / 8.0, 50.0 / 8.0, 34.0 / 8.0},
+                                  {120.0 / 20.0, 90.0 / 20.0, 50.0 / 20.0}};
+  const hst_gpu_params& p = ctx->p;
+  const bool damp = damping_active(p);
+  for (int i = 0; i < 3; ++i) {
+    const double* ODE = RK[i];
+    const double t = *time;
+    if (!p.linear || i == 2) {
+      if (i == 2) CK(cudaMemsetAsync(ctx->d.cfl, 0, sizeof(unsigned long long), ctx->stream));
+      CK(timed(ctx, HST_KC_ZINV, [&] { return hst::launch_zinv(ctx->g, ctx->d, ctx->stream); }));
+      CK(timed(ctx, HST_KC_XPROD, [&] { return hst::launch_xprod(ctx->g, ctx->d, ctx->ps, i == 2, ctx->stream); }));
+      if (!p.linear) CK(timed(ctx, HST_KC_ZFWD, [&] { return hst::launch_zfwd(ctx->g, ctx->d, ctx->stream); }));
+    }
+    if (damp && damping_update(ctx, t)) {
+      // stream-ordered upload of the new table (the previous copy has been
+      // consumed once the stream reaches it, so wait before refilling)
+      CK(cudaStreamSynchronize(ctx->stream));
+      std::memcpy(ctx->h_gdamp, ctx->gdamp.data(), sizeof(double) * ctx->g.ncol);
+      CK(cudaMemcpyAsync(ctx->d.gdamp, ctx->h_gdamp, sizeof(double) * ctx->g.ncol, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    SubstepScalars sc;
+    sc.ode0 = ODE[0];
+    sc.ode1 = ODE[1];
+    sc.ode2 = ODE[2];
+    sc.deltat = deltat;
+    const double dt_sub = 2.0 / ODE[0] * deltat;
+    sc.lambda = ODE[0] / deltat;
+    sc.s2now = s2_of(p, t);
+    sc.gsoft = (damp && !p.damp_hard) ? 1.0 : 0.0;
+    sc.damp_hard = (p.damp_hard && damp) ? 1 : 0;
+    sc.dgx = p.S * dt_sub;
+    sc.dgz = s2_integral(p, t, t + dt_sub);
+    shear_shifts(ctx, t, &sc.sx_t, &sc.sz_t);
+    shear_shifts(ctx, t + dt_sub, &sc.sx_n, &sc.sz_n);
+    CK(timed(ctx, HST_KC_COLUMN,
+             [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, ctx->stream); }));
+    *time = t + dt_sub;
+  }
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_timestep(hst_ctx* ctx, double* time, double deltat, double* cfl) {
+  if (!ctx || !time) return HST_EARG;
+  CK(cudaSetDevice(ctx->device));
+  int rc = queue_timestep(ctx, time, deltat);
+  if (rc != HST_OK) return rc;
+  return read_cfl(ctx, cfl);
+}
+
+extern "C" int hst_gpu_timesteps(hst_ctx* ctx, int n, double* time, double deltat) {
+  if (!ctx || !time || n < 0) return HST_EARG;
+  CK(cudaSetDevice(ctx->device));
+  for (int k = 0; k < n; ++k) {
+    int rc = queue_timestep(ctx, time, deltat);
+    if (rc != HST_OK) return rc;
+  }
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_set_profiling(hst_ctx* ctx, int on) {
+  if (!ctx) return HST_EARG;
+  ctx->prof_on = on != 0;
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_kernel_times(hst_ctx* ctx, double* ms, long long* count) {
+  if (!ctx) return HST_EARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (size_t k = 0; k < ctx->ev_class.size(); ++k) {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, ctx->ev[2 * k], ctx->ev[2 * k + 1]));
+    ctx->prof_ms[ctx->ev_class[k]] += t;
+    ctx->prof_n[ctx->ev_class[k]] += 1;
+  }
+  ctx->ev_class.clear();
+  for (int k = 0; k < HST_KC_N; ++k) {
+    if (ms) ms[k] = ctx->prof_ms[k];
+    if (count) count[k] = ctx->prof_n[k];
+  }
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_reset_kernel_times(hst_ctx* ctx) {
+  if (!ctx) return HST_EARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->ev_class.clear();
+  for (int k = 0; k < HST_KC_N; ++k) {
+    ctx->prof_ms[k] = 0.0;
+    ctx->prof_n[k] = 0;
+  }
+  return HST_OK;
+}

@@ -1,0 +1,393 @@
+// Device building blocks of the hst substep on sm_100a: complex FP64
+// arithmetic, the compact-stencil coefficients, the warp-group cyclic
+// pentadiagonal line solver and the shared-memory Stockham FFT.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hst {
+
+// ------------------------------------------------------------ complex ----
+typedef double2 cxd;
+__device__ __forceinline__ cxd mkc(double r, double i) { return make_double2(r, i); }
+__device__ __forceinline__ cxd cadd(cxd a, cxd b) { return mkc(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ cxd csub(cxd a, cxd b) { return mkc(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ cxd cmul(cxd a, cxd b) { return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ cxd cscale(double s, cxd a) { return mkc(s * a.x, s * a.y); }
+__device__ __forceinline__ cxd cconj(cxd a) { return mkc(a.x, -a.y); }
+__device__ __forceinline__ cxd cneg(cxd a) { return mkc(-a.x, -a.y); }
+// (0 + i b) * a
+__device__ __forceinline__ cxd cmuli(double b, cxd a) { return mkc(-b * a.y, b * a.x); }
+// a - s * b (s real)
+__device__ __forceinline__ cxd cfms(cxd a, double s, cxd b) { return mkc(a.x - s * b.x, a.y - s * b.y); }
+__device__ __forceinline__ cxd cdivr(cxd a, double d) { return mkc(a.x / d, a.y / d); }
+__device__ __forceinline__ cxd cexpi(double x) {
+  double s, c;
+  sincos(x, &s, &c);
+  return mkc(c, s);
+}
+// complex division with range reduction (Smith)
+__device__ __forceinline__ cxd cdiv(cxd a, cxd b) {
+  if (fabs(b.x) >= fabs(b.y)) {
+    double r = b.y / b.x, d = b.x + b.y * r;
+    return mkc((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+  } else {
+    double r = b.x / b.y, d = b.x * r + b.y;
+    return mkc((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+  }
+}
+__device__ __forceinline__ double shfl_d(unsigned mask, double v, int src, int width) {
+  return __shfl_sync(mask, v, src, width);
+}
+__device__ __forceinline__ cxd shfl_c(unsigned mask, cxd v, int src, int width) {
+  return mkc(__shfl_sync(mask, v.x, src, width), __shfl_sync(mask, v.y, src, width));
+}
+
+// line-solve kinds (src/hst_linsolve.f90:83)
+enum { K_D2V = 1, K_ETA = 2, K_POISSON = 3, K_D0 = 4, K_DY = 5 };
+
+// der(iy, n, j), n = 0..3 (D0, D1, D2, D4), j = -2..2; Fortran order
+// der(0:ny-1, 0:3, -2:2) as set up by src/hst_derivatives.f90:30-56.
+__device__ __forceinline__ double derv(const double* __restrict__ der, int ny, int iy, int n, int j) {
+  return __ldg(der + iy + ny * (n + 4 * (j + 2)));
+}
+
+// The five band entries of row iy of system `sys` before the wrap phase:
+// coef, src/hst_linsolve.f90:236-252.
+__device__ __forceinline__ void row_coefs(int sys, double lambda, double ni, double kk, const double* __restrict__ der,
+                                          int ny, int iy, double a[5]) {
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    double d0 = derv(der, ny, iy, 0, j - 2);
+    if (sys == K_D2V) {
+      double d2 = derv(der, ny, iy, 2, j - 2), d4 = derv(der, ny, iy, 3, j - 2);
+      a[j] = lambda * (d2 - kk * d0) - ni * (d4 - 2.0 * kk * d2 + kk * kk * d0);
+    } else if (sys == K_ETA) {
+      double d2 = derv(der, ny, iy, 2, j - 2);
+      a[j] = lambda * d0 - ni * (d2 - kk * d0);
+    } else if (sys == K_POISSON) {
+      double d2 = derv(der, ny, iy, 2, j - 2);
+      a[j] = d2 - kk * d0;
+    } else {
+      a[j] = d0;
+    }
+  }
+}
+__device__ __forceinline__ double row_coef(int sys, double lambda, double ni, double kk, const double* __restrict__ der,
+                                           int ny, int iy, int j) {
+  double d0 = derv(der, ny, iy, 0, j);
+  if (sys == K_D2V) {
+    double d2 = derv(der, ny, iy, 2, j), d4 = derv(der, ny, iy, 3, j);
+    return lambda * (d2 - kk * d0) - ni * (d4 - 2.0 * kk * d2 + kk * kk * d0);
+  } else if (sys == K_ETA) {
+    double d2 = derv(der, ny, iy, 2, j);
+    return lambda * d0 - ni * (d2 - kk * d0);
+  } else if (sys == K_POISSON) {
+    return derv(der, ny, iy, 2, j) - kk * d0;
+  }
+  return d0;
+}
+
+// ------------------------------------------------ 2x2 block helpers ----
+struct M2 {
+  double a, b, c, d;  // [[a, b], [c, d]]
+};
+__device__ __forceinline__ M2 m2inv(M2 m) {
+  double det = m.a * m.d - m.b * m.c;
+  double r = 1.0 / det;
+  M2 o = {m.d * r, -m.b * r, -m.c * r, m.a * r};
+  return o;
+}
+__device__ __forceinline__ M2 m2mul(M2 x, M2 y) {
+  M2 o = {x.a * y.a + x.b * y.c, x.a * y.b + x.b * y.d, x.c * y.a + x.d * y.c, x.c * y.b + x.d * y.d};
+  return o;
+}
+__device__ __forceinline__ M2 m2sub(M2 x, M2 y) {
+  M2 o = {x.a - y.a, x.b - y.b, x.c - y.c, x.d - y.d};
+  return o;
+}
+__device__ __forceinline__ M2 m2neg(M2 x) {
+  M2 o = {-x.a, -x.b, -x.c, -x.d};
+  return o;
+}
+struct V2c {
+  cxd u, v;
+};
+__device__ __forceinline__ V2c m2vec(M2 m, V2c x) {
+  V2c o = {mkc(m.a * x.u.x + m.b * x.v.x, m.a * x.u.y + m.b * x.v.y),
+           mkc(m.c * x.u.x + m.d * x.v.x, m.c * x.u.y + m.d * x.v.y)};
+  return o;
+}
+__device__ __forceinline__ V2c v2sub(V2c x, V2c y) {
+  V2c o = {csub(x.u, y.u), csub(x.v, y.v)};
+  return o;
+}
+__device__ __forceinline__ V2c v2scale(cxd s, V2c x) {
+  V2c o = {cmul(s, x.u), cmul(s, x.v)};
+  return o;
+}
+// complex 2x2
+struct C2 {
+  cxd a, b, c, d;
+};
+__device__ __forceinline__ C2 c2_from(M2 m) {
+  C2 o = {mkc(m.a, 0), mkc(m.b, 0), mkc(m.c, 0), mkc(m.d, 0)};
+  return o;
+}
+__device__ __forceinline__ C2 c2_axpby(M2 x, cxd s, M2 y, cxd t) {  // x s + y t
+  C2 o = {cadd(cscale(x.a, s), cscale(y.a, t)), cadd(cscale(x.b, s), cscale(y.b, t)),
+          cadd(cscale(x.c, s), cscale(y.c, t)), cadd(cscale(x.d, s), cscale(y.d, t))};
+  return o;
+}
+__device__ __forceinline__ C2 c2mul_cr(C2 x, M2 y) {  // complex x real
+  C2 o = {cadd(cscale(y.a, x.a), cscale(y.c, x.b)), cadd(cscale(y.b, x.a), cscale(y.d, x.b)),
+          cadd(cscale(y.a, x.c), cscale(y.c, x.d)), cadd(cscale(y.b, x.c), cscale(y.d, x.d))};
+  return o;
+}
+__device__ __forceinline__ C2 c2mul(C2 x, C2 y) {
+  C2 o = {cadd(cmul(x.a, y.a), cmul(x.b, y.c)), cadd(cmul(x.a, y.b), cmul(x.b, y.d)),
+          cadd(cmul(x.c, y.a), cmul(x.d, y.c)), cadd(cmul(x.c, y.b), cmul(x.d, y.d))};
+  return o;
+}
+__device__ __forceinline__ V2c c2vec(C2 m, V2c x) {
+  V2c o = {cadd(cmul(m.a, x.u), cmul(m.b, x.v)), cadd(cmul(m.c, x.u), cmul(m.d, x.v))};
+  return o;
+}
+// solve m z = r for complex 2x2 m
+__device__ __forceinline__ V2c c2solve(C2 m, V2c r) {
+  cxd det = csub(cmul(m.a, m.d), cmul(m.b, m.c));
+  cxd n1 = csub(cmul(m.d, r.u), cmul(m.b, r.v));
+  cxd n2 = csub(cmul(m.a, r.v), cmul(m.c, r.u));
+  V2c o = {cdiv(n1, det), cdiv(n2, det)};
+  return o;
+}
+__device__ __forceinline__ M2 shfl_m2(unsigned mask, M2 m, int src, int w) {
+  M2 o = {shfl_d(mask, m.a, src, w), shfl_d(mask, m.b, src, w), shfl_d(mask, m.c, src, w), shfl_d(mask, m.d, src, w)};
+  return o;
+}
+__device__ __forceinline__ V2c shfl_v2(unsigned mask, V2c v, int src, int w) {
+  V2c o = {shfl_c(mask, v.u, src, w), shfl_c(mask, v.v, src, w)};
+  return o;
+}
+__device__ __forceinline__ C2 shfl_c2(unsigned mask, C2 m, int src, int w) {
+  C2 o = {shfl_c(mask, m.a, src, w), shfl_c(mask, m.b, src, w), shfl_c(mask, m.c, src, w), shfl_c(mask, m.d, src, w)};
+  return o;
+}
+
+// ------------------------------------------------- line buffer layout ----
+// A line of n = P*m rows lives in shared memory slab by slab: slab s (the
+// rows s*m .. s*m+m-1 owned by lane s of the group) starts at s*MS with
+// MS = m rounded up to odd, so that the P lanes reading their own slab at
+// the same offset hit different 16-byte bank groups.
+struct LineGeom {
+  int n, m, MS, P;
+  unsigned invm;  // ceil(2^20 / m): r / m for r * m < 2^20
+  __device__ __forceinline__ int slab(int r) const { return (int)(((unsigned)r * invm) >> 20); }
+  __device__ __forceinline__ int at(int r) const {
+    int s = slab(r);
+    return s * MS + (r - s * m);
+  }
+};
+
+// ------------------------------------------- the warp-group line solve ----
+// One cyclic pentadiagonal system per line, solved by a group of P lanes
+// (P a power of two, 2..32), lane s owning the slab of rows s*m..s*m+m-1.
+// The algorithm is the reference's multi-slab bordering
+// (src/hst_linsolve.f90:1-64, penta_forward :282-354, the reduced system of
+// penta_backward :377-435) with every lane a slab: each lane factors its
+// slab interior (real arithmetic, complex right-hand side) and writes the
+// 28-value record; the 2P border unknowns then satisfy a block-cyclic
+// tridiagonal system with 2x2 blocks.  Instead of dense Gaussian
+// elimination over all slabs, that system is solved by parallel cyclic
+// reduction across the lanes.  The wrap phase ph = exp(-i theta) enters only
+// through the box edge; with b_s = mu^s c_s, mu = exp(-i theta/P), every
+// block becomes real and the phase a uniform factor mu^(-1) (below) and mu
+// (above), so the reduction runs on real 2x2 blocks with a complex
+// right-hand side.  The back substitution then runs per slab
+// (penta_backward :461-482).
+//
+// buf: the line (right-hand side in, solution out), in LineGeom layout.
+// fac: per-lane factor scratch, (m-2) x 4 x P doubles.
+// Rows of the right-hand side of KIND_DY must already hold D1 src.
+template <int P>
+__device__ void group_solve(int sys, double lambda, double ni, double kk, double theta, const double* __restrict__ der,
+                            int ny, const LineGeom& G, cxd* buf, double* fac, int s, unsigned gmask) {
+  const int m = G.m, mi = m - 2, MS = G.MS;
+  const int r0 = s * m;
+  cxd* sb = buf + s * MS;
+  // ---- forward sweep of the slab interior (penta_forward)
+  double u11 = 0, u12 = 0, p1 = 0, q1 = 0, u21 = 0, u22 = 0, p2 = 0, q2 = 0;
+  double w1 = 0, w2 = 0, v1 = 0, v2 = 0, sp0 = 0, sq0 = 0, sp1 = 0, sq1 = 0;
+  cxd x1 = mkc(0, 0), x2 = mkc(0, 0), sx0 = mkc(0, 0), sx1 = mkc(0, 0);
+  for (int i = 0; i < mi; ++i) {
+    double a[5];
+    row_coefs(sys, lambda, ni, kk, der, ny, r0 + i, a);
+    double p = 0, q = 0;
+    if (i == 0) {
+      p = a[0];
+      q = a[1];
+    }
+    if (i == 1) q = a[0];
+    cxd bx = sb[i];
+    if (i >= 2) {
+      double l = a[0];
+      a[1] = a[1] - l * u21;
+      a[2] = a[2] - l * u22;
+      bx = cfms(bx, l, x2);
+      p = p - l * p2;
+      q = q - l * q2;
+    }
+    if (i >= 1) {
+      double l = a[1];
+      a[2] = a[2] - l * u11;
+      a[3] = a[3] - l * u12;
+      bx = cfms(bx, l, x1);
+      p = p - l * p1;
+      q = q - l * q1;
+    }
+    double rp = 1.0 / a[2];
+    double t1 = a[3] * rp, t2 = a[4] * rp;
+    bx = cscale(rp, bx);
+    p = p * rp;
+    q = q * rp;
+    fac[(i * 4 + 0) * P + s] = t1;
+    fac[(i * 4 + 1) * P + s] = t2;
+    fac[(i * 4 + 2) * P + s] = p;
+    fac[(i * 4 + 3) * P + s] = q;
+    sb[i] = bx;
+    double w = (i == 0) ? 1.0 : -(u11 * w1 + u22 * w2);
+    double v = (i == 1) ? 1.0 : -(u11 * v1 + u22 * v2);
+    sx0 = mkc(sx0.x + w * bx.x, sx0.y + w * bx.y);
+    sp0 = sp0 + w * p;
+    sq0 = sq0 + w * q;
+    sx1 = mkc(sx1.x + v * bx.x, sx1.y + v * bx.y);
+    sp1 = sp1 + v * p;
+    sq1 = sq1 + v * q;
+    w2 = w1;
+    w1 = w;
+    v2 = v1;
+    v1 = v;
+    u21 = u11;
+    u22 = u12;
+    x2 = x1;
+    p2 = p1;
+    q2 = q1;
+    u11 = t1;
+    u12 = t2;
+    x1 = bx;
+    p1 = p;
+    q1 = q;
+  }
+  // the record of the slab (rec(1..28) of penta_forward)
+  const cxd X0 = sx0;
+  const double R3 = sp0, R4 = sq0, R5 = w2 * u22 + w1 * u11, R6 = w1 * u12;
+  const cxd X1 = sx1;
+  const double R9 = sp1, R10 = sq1, R11 = v2 * u22 + v1 * u11, R12 = v1 * u12;
+  const cxd XM2 = csub(x2, cscale(u21, x1));
+  const double R15 = p2 - u21 * p1, R16 = q2 - u21 * q1, R17 = u22 - u21 * u11, R18 = -u21 * u12;
+  const cxd XM1 = x1;
+  const double R21 = p1, R22 = q1, R23 = u11, R24 = u12;
+  const cxd RB1 = sb[mi], RB2 = sb[mi + 1];
+  // rows 0, 1 of the slab above (t = s+1)
+  const int t = (s + 1) & (P - 1);
+  const cxd TX0 = shfl_c(gmask, X0, t, P), TX1 = shfl_c(gmask, X1, t, P);
+  const double T3 = shfl_d(gmask, R3, t, P), T4 = shfl_d(gmask, R4, t, P), T5 = shfl_d(gmask, R5, t, P),
+               T6 = shfl_d(gmask, R6, t, P), T9 = shfl_d(gmask, R9, t, P), T10 = shfl_d(gmask, R10, t, P),
+               T11 = shfl_d(gmask, R11, t, P), T12 = shfl_d(gmask, R12, t, P);
+  // the two border rows of the slab (global rows ga, ga+1)
+  const int ga = r0 + mi;
+  const double c1m4 = row_coef(sys, lambda, ni, kk, der, ny, ga, -2), c1m3 = row_coef(sys, lambda, ni, kk, der, ny, ga, -1);
+  const double d11 = row_coef(sys, lambda, ni, kk, der, ny, ga, 0), d12 = row_coef(sys, lambda, ni, kk, der, ny, ga, 1);
+  const double c10 = row_coef(sys, lambda, ni, kk, der, ny, ga, 2);
+  const double c2m3 = row_coef(sys, lambda, ni, kk, der, ny, ga + 1, -2), d21 = row_coef(sys, lambda, ni, kk, der, ny, ga + 1, -1);
+  const double d22 = row_coef(sys, lambda, ni, kk, der, ny, ga + 1, 0), c20 = row_coef(sys, lambda, ni, kk, der, ny, ga + 1, 1);
+  const double c21 = row_coef(sys, lambda, ni, kk, der, ny, ga + 1, 2);
+  // phases: ph = exp(-i theta) across the box edge; mu = ph^(1/P)
+  const cxd ph = cexpi(-theta);
+  const cxd mu = cexpi(-(theta / (double)P));
+  // mu^s by binary powering (consistent with the squarings below)
+  cxd mus = mkc(1.0, 0.0);
+  {
+    cxd b = mu;
+    for (int e = s; e; e >>= 1) {
+      if (e & 1) mus = cmul(mus, b);
+      b = cmul(b, b);
+    }
+  }
+  const cxd php = (s == P - 1) ? ph : mkc(1.0, 0.0);
+  // block row s: L mu^-1 c_{s-1} + D c_s + U mu c_{s+1} = r mu^-s
+  M2 L = {-(c1m4 * R15 + c1m3 * R21), -(c1m4 * R16 + c1m3 * R22), -(c2m3 * R21), -(c2m3 * R22)};
+  M2 D = {d11 - (c1m4 * R17 + c1m3 * R23) - c10 * T3, d12 - (c1m4 * R18 + c1m3 * R24) - c10 * T4,
+          d21 - c2m3 * R23 - (c20 * T3 + c21 * T9), d22 - c2m3 * R24 - (c20 * T4 + c21 * T10)};
+  M2 U = {-(c10 * T5), -(c10 * T6), -(c20 * T5 + c21 * T11), -(c20 * T6 + c21 * T12)};
+  V2c r;
+  {
+    cxd b1 = csub(csub(csub(RB1, cscale(c1m4, XM2)), cscale(c1m3, XM1)), cmul(cscale(c10, php), TX0));
+    cxd b2 = csub(csub(RB2, cscale(c2m3, XM1)),
+                  cmul(php, mkc(c20 * TX0.x + c21 * TX1.x, c20 * TX0.y + c21 * TX1.y)));
+    V2c rr = {b1, b2};
+    r = v2scale(cconj(mus), rr);
+  }
+  // parallel cyclic reduction: strides d = 1, 2, .., P/4
+  cxd mud = mu;  // mu^d
+  for (int d = 1; 2 * d < P; d <<= 1) {
+    const int sm = (s - d) & (P - 1), sp = (s + d) & (P - 1);
+    M2 Lm = shfl_m2(gmask, L, sm, P), Dm = shfl_m2(gmask, D, sm, P), Um = shfl_m2(gmask, U, sm, P);
+    M2 Lp = shfl_m2(gmask, L, sp, P), Dp = shfl_m2(gmask, D, sp, P), Up = shfl_m2(gmask, U, sp, P);
+    V2c rm = shfl_v2(gmask, r, sm, P), rpv = shfl_v2(gmask, r, sp, P);
+    M2 A = m2mul(L, m2inv(Dm));
+    M2 Gm = m2mul(U, m2inv(Dp));
+    M2 Ln = m2neg(m2mul(A, Lm));
+    M2 Un = m2neg(m2mul(Gm, Up));
+    M2 Dn = m2sub(m2sub(D, m2mul(A, Um)), m2mul(Gm, Lp));
+    V2c ta = v2scale(cconj(mud), m2vec(A, rm));
+    V2c tg = v2scale(mud, m2vec(Gm, rpv));
+    r = v2sub(v2sub(r, ta), tg);
+    L = Ln;
+    U = Un;
+    D = Dn;
+    mud = cmul(mud, mud);
+  }
+  // last level: c_{s-P/2} = c_{s+P/2}; pair with lane s ^ P/2
+  V2c c;
+  {
+    C2 Mx = c2_axpby(L, cconj(mud), U, mud);
+    const int q = s ^ (P >> 1);
+    M2 Dq = shfl_m2(gmask, D, q, P);
+    C2 Mq = shfl_c2(gmask, Mx, q, P);
+    V2c rq = shfl_v2(gmask, r, q, P);
+    C2 X = c2mul_cr(Mx, m2inv(Dq));
+    C2 Sc = c2mul(X, Mq);
+    C2 Dc = c2_from(D);
+    Sc.a = csub(Dc.a, Sc.a);
+    Sc.b = csub(Dc.b, Sc.b);
+    Sc.c = csub(Dc.c, Sc.c);
+    Sc.d = csub(Dc.d, Sc.d);
+    V2c rhs = v2sub(r, c2vec(X, rq));
+    c = c2solve(Sc, rhs);
+  }
+  // the border of this slab and of the slab below
+  const cxd xb1 = cmul(mus, c.u), xb2 = cmul(mus, c.v);
+  const int sb_ = (s - 1) & (P - 1);
+  cxd yb1 = shfl_c(gmask, xb1, sb_, P), yb2 = shfl_c(gmask, xb2, sb_, P);
+  if (s == 0) {
+    yb1 = cmul(cconj(ph), yb1);
+    yb2 = cmul(cconj(ph), yb2);
+  }
+  sb[mi] = xb1;
+  sb[mi + 1] = xb2;
+  // back substitution (penta_backward :467-482)
+  cxd xk1 = xb1, xk2 = xb2;
+  for (int i = mi - 1; i >= 0; --i) {
+    double U1 = fac[(i * 4 + 0) * P + s], U2 = fac[(i * 4 + 1) * P + s];
+    double B1 = fac[(i * 4 + 2) * P + s], B2 = fac[(i * 4 + 3) * P + s];
+    cxd xr = sb[i];
+    cxd xk = mkc(xr.x - B1 * yb1.x - B2 * yb2.x - U1 * xk1.x - U2 * xk2.x,
+                 xr.y - B1 * yb1.y - B2 * yb2.y - U1 * xk1.y - U2 * xk2.y);
+    sb[i] = xk;
+    xk2 = xk1;
+    xk1 = xk;
+  }
+}
+
+}  // namespace hst

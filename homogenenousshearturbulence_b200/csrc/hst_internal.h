@@ -1,0 +1,63 @@
+// Internal interface between the C ABI (hst_capi.cu) and the kernels
+// (hst_kernels.cu).  Not installed; the public interface is include/hst_gpu.h.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/hst_gpu.h"
+
+namespace hst {
+
+// Sizes and device pointers of one field: everything a launch needs.
+struct Geometry {
+  int nx, ny, nz;      // deck sizes
+  int nxd, nzd;        // padded transform sizes (2 nxd physical x points, nzd z points)
+  int nxB, nzT, rows;  // nx+1, 2nz+1, ny+4
+  int ncol;            // nxB * nzT Fourier columns
+  long nf;             // complex elements of one field (ncol * rows)
+  int P, m, MS;        // line-solve group: P lanes, m rows per lane, slab stride
+  int Ty;              // y tile of the transforms (divides ny)
+  int ppt;             // FFT points per thread
+};
+
+struct DeviceState {
+  double2* F[7];        // V1 V2 V3 OLD1 OLD2 RHS1 RHS2, (iy fastest, ghost rows included)
+  double2* Z;           // z-inverse of V: [3][nzd][ny/Ty][nxB][Ty]
+  double2* Pp;          // x-forward of the products: [6][nzd][ny/Ty][nxB][Ty]
+  double2* Q;           // spectral products: [6][ncol][ny]
+  double* der;          // der(0:ny-1, 0:3, -2:2)
+  double* y;            // y(-2:ny+1)
+  double* dyl;          // dyl(0:ny-1)
+  double* gdamp;        // gdamp(-nz:nz, 0:nx)
+  double2* twx;         // exp(-2 pi i e / (2 nxd))
+  double2* twz;         // exp(-2 pi i e / nzd)
+  unsigned long long* cfl;  // running max (bits of a non-negative double)
+};
+
+// Scalars of one substep of the column kernel.
+struct SubstepScalars {
+  double ode0, ode1, ode2, deltat, lambda;
+  double s2now, gsoft;
+  double dgx, dgz;
+  double sx_t, sz_t;  // wrap displacements at t
+  double sx_n, sz_n;  // at t + dt_sub
+  int damp_hard;
+};
+
+struct PhysScalars {
+  double alfa0, beta0, ni, S;
+  double dx, dz, factor;
+};
+
+cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st);
+cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int want_cfl, cudaStream_t st);
+cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st);
+cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysScalars& ph, const SubstepScalars& sc,
+                          int exact, int nonlin, cudaStream_t st);
+cudaError_t launch_line_solve(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int sys, double lambda,
+                              int src, int dst, double sx, double sz, cudaStream_t st);
+cudaError_t launch_fill_ghosts(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int field, double sx,
+                               double sz, cudaStream_t st);
+size_t column_smem_bytes(const Geometry& g, int exact);
+
+}  // namespace hst

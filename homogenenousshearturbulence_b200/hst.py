@@ -1,0 +1,409 @@
+"""Python host side of the hst substep on a B200: a thin ctypes binding of the
+C ABI in include/hst_gpu.h (libhst_gpu.so, built in this directory), with the
+names and argument meanings of the reference's Fortran interfaces:
+
+  Solver.timestep()                          hst_equations::timestep (src/hst_equations.f90:56-87)
+  Solver.line_solve(kind, lam, src, dst)     hst_linsolve::line_solve (src/hst_linsolve.f90:147-233)
+  Solver.fill_ghosts(field[, sx, sz])        hst_derivatives::fill_ghosts[_field] (:134-157)
+  Solver.compute_cfl()                       hst_transforms::compute_cfl (src/hst_transforms.f90:163-179)
+  Solver.shear_shifts(t), s2_of, s2_integral hst_derivatives (:85-128)
+
+Fields are numpy complex128 arrays of shape (nx+1, 2nz+1, ny+4), i.e. the
+reference's V(iy, iz, ix) with iy fastest.  There is no CPU fallback: the
+library must be built (build.py) and a CUDA device present.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import math
+import pathlib
+
+import numpy as np
+
+PKG = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG / "libhst_gpu.so"
+
+V1, V2, V3, OLD1, OLD2, RHS1, RHS2 = range(7)
+KIND_D2V, KIND_ETA, KIND_POISSON, KIND_D0, KIND_DY = 1, 2, 3, 4, 5
+# RK_rai (src/hst_params.f90:108-111), one row per substep
+RK_RAI = ((120.0 / 32.0, 2.0, 0.0), (120.0 / 8.0, 50.0 / 8.0, 34.0 / 8.0), (120.0 / 20.0, 90.0 / 20.0, 50.0 / 20.0))
+PI = 3.141592653589793
+
+
+class HstError(RuntimeError):
+    pass
+
+
+class Params(ct.Structure):
+    """hst_gpu_params (include/hst_gpu.h)."""
+    _fields_ = [
+        ("nx", ct.c_int), ("ny", ct.c_int), ("nz", ct.c_int),
+        ("nxd", ct.c_int), ("nzd", ct.c_int),
+        ("alfa0", ct.c_double), ("beta0", ct.c_double), ("ly", ct.c_double), ("ystretch", ct.c_double),
+        ("re", ct.c_double), ("S", ct.c_double),
+        ("linear", ct.c_int), ("exact_shift", ct.c_int),
+        ("s2_mean", ct.c_double), ("s2_amplitude", ct.c_double), ("s2_period", ct.c_double), ("s2_start", ct.c_double),
+        ("damp_kpar", ct.c_double), ("damp_kperp", ct.c_double), ("damp_rate", ct.c_double),
+        ("damp_edge", ct.c_double), ("damp_norm", ct.c_double), ("damp_angle", ct.c_double),
+        ("damp_hard", ct.c_int), ("damp_mean", ct.c_int), ("damp_follow", ct.c_int),
+        ("device", ct.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libhst_gpu.so; raises if it is missing (no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise HstError(f"{LIB_PATH} is missing: build it with `python -m homogenenousshearturbulence_b200.build`")
+        L = ct.CDLL(str(LIB_PATH))
+        P = ct.POINTER
+        d, i, vp = ct.c_double, ct.c_int, ct.c_void_p
+        sig = {
+            "hst_gpu_create": (i, [P(Params), P(vp)]),
+            "hst_gpu_destroy": (i, [vp]),
+            "hst_gpu_last_error": (ct.c_char_p, [vp]),
+            "hst_gpu_device_bytes": (d, [P(Params)]),
+            "hst_gpu_set_tables": (i, [vp, P(d), P(d), P(d)]),
+            "hst_gpu_get_tables": (i, [vp, P(d), P(d), P(d)]),
+            "hst_gpu_upload": (i, [vp, i, P(d)]),
+            "hst_gpu_download": (i, [vp, i, P(d)]),
+            "hst_gpu_timestep": (i, [vp, P(d), d, P(d)]),
+            "hst_gpu_timesteps": (i, [vp, i, P(d), d]),
+            "hst_gpu_line_solve": (i, [vp, i, d, i, i, i, d, d, d]),
+            "hst_gpu_fill_ghosts": (i, [vp, i, d, d]),
+            "hst_gpu_fill_ghosts_at": (i, [vp, i, d]),
+            "hst_gpu_compute_cfl": (i, [vp, P(d)]),
+            "hst_gpu_sync": (i, [vp]),
+            "hst_gpu_shear_shifts": (i, [vp, d, P(d), P(d)]),
+            "hst_gpu_s2_of": (d, [vp, d]),
+            "hst_gpu_s2_integral": (d, [vp, d, d]),
+            "hst_gpu_launch_count": (ct.c_longlong, [vp]),
+            "hst_gpu_set_profiling": (i, [vp, i]),
+            "hst_gpu_kernel_times": (i, [vp, P(d), P(ct.c_longlong)]),
+            "hst_gpu_reset_kernel_times": (i, [vp]),
+            "hst_gpu_stream": (vp, [vp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+# ------------------------------------------------------------------ deck ----
+DECK_DEFAULTS = dict(  # src/hst_input.f90:140-155
+    nx=63, ny=128, nz=63, alfa0=2.0 * PI / 3.0, beta0=2.0 * PI, ly=2.0, ystretch=0.0,
+    re=1000.0, S=1.0, linear=False, exact_shift=False,
+    s2_mean=0.0, s2_amplitude=0.0, s2_period=0.0, s2_start=0.0,
+    deltat=0.0, cflmax=1.0, t_max=100.0, nstep=1000000, time=0.0,
+    amplitude=1.0e-3, seed=1, kpeak=4.0,
+    damp_kpar=0.0, damp_kperp=0.0, damp_rate=0.0, damp_hard=False, damp_edge=0.0, damp_norm=2.0,
+    damp_mean=False, damp_follow=True, damp_angle=0.0,
+)
+
+
+def read_deck(path) -> dict:
+    """Reads the namelist groups of an hst.in deck (the subset the path uses)."""
+    text = []
+    for line in pathlib.Path(path).read_text().splitlines():
+        out, q = [], None
+        for ch in line:
+            if ch in "'\"":
+                q = None if q == ch else (ch if q is None else q)
+            if ch == "!" and q is None:
+                break
+            out.append(ch)
+        text.append("".join(out))
+    body = "\n".join(text)
+    deck = dict(DECK_DEFAULTS)
+    keys = {k.lower(): k for k in deck}
+    for grp in body.split("&")[1:]:
+        grp = grp.split("/")[0]
+        parts = grp.split(None, 1)
+        if len(parts) < 2:
+            continue
+        items = parts[1]
+        import re as _re
+        for m in _re.finditer(r"([A-Za-z_][A-Za-z0-9_]*)\s*=\s*('[^']*'|\"[^\"]*\"|[^,\n]+)", items):
+            k, v = m.group(1).lower(), m.group(2).strip()
+            if k not in keys:
+                continue
+            name = keys[k]
+            ref = DECK_DEFAULTS[name]
+            if isinstance(ref, bool):
+                deck[name] = v.lower().strip(".") in ("true", "t")
+            elif isinstance(ref, int):
+                deck[name] = int(float(v.replace("d", "e").replace("D", "e")))
+            elif isinstance(ref, float):
+                deck[name] = float(v.replace("d", "e").replace("D", "e"))
+            else:
+                deck[name] = v.strip("'\"")
+    return deck
+
+
+# --------------------------------------------------------------- solver ----
+class Solver:
+    """One field resident on one GPU (one hst_ctx)."""
+
+    def __init__(self, deck: dict | None = None, device: int = 0, **kw):
+        cfg = dict(DECK_DEFAULTS)
+        if deck:
+            cfg.update(deck)
+        cfg.update(kw)
+        self.cfg = cfg
+        p = Params()
+        p.nx, p.ny, p.nz = int(cfg["nx"]), int(cfg["ny"]), int(cfg["nz"])
+        p.nxd, p.nzd = int(cfg.get("nxd", 0)), int(cfg.get("nzd", 0))
+        p.alfa0, p.beta0, p.ly, p.ystretch = cfg["alfa0"], cfg["beta0"], cfg["ly"], cfg["ystretch"]
+        p.re, p.S = cfg["re"], cfg["S"]
+        p.linear, p.exact_shift = int(bool(cfg["linear"])), int(bool(cfg["exact_shift"]))
+        p.s2_mean, p.s2_amplitude = cfg["s2_mean"], cfg["s2_amplitude"]
+        p.s2_period, p.s2_start = cfg["s2_period"], cfg["s2_start"]
+        p.damp_kpar, p.damp_kperp, p.damp_rate = cfg["damp_kpar"], cfg["damp_kperp"], cfg["damp_rate"]
+        p.damp_edge, p.damp_norm, p.damp_angle = cfg["damp_edge"], cfg["damp_norm"], cfg["damp_angle"]
+        p.damp_hard, p.damp_mean, p.damp_follow = int(bool(cfg["damp_hard"])), int(bool(cfg["damp_mean"])), int(
+            bool(cfg["damp_follow"]))
+        p.device = int(device)
+        self.params = p
+        self._h = ct.c_void_p()
+        rc = lib().hst_gpu_create(ct.byref(p), ct.byref(self._h))
+        if rc != 0:
+            raise HstError(f"hst_gpu_create failed ({rc}) for nx={p.nx} ny={p.ny} nz={p.nz}")
+        self.nx, self.ny, self.nz = p.nx, p.ny, p.nz
+        self.nxd, self.nzd = p.nxd, p.nzd
+        self.shape = (self.nx + 1, 2 * self.nz + 1, self.ny + 4)
+        self.time = float(cfg.get("time", 0.0))
+        self.deltat = float(cfg.get("deltat", 0.0))
+        self.cfl = 0.0
+        self._tables()
+
+    def _tables(self):
+        ny = self.ny
+        der = np.zeros(20 * ny)
+        y = np.zeros(ny + 4)
+        dyl = np.zeros(ny)
+        P = ct.POINTER(ct.c_double)
+        lib().hst_gpu_get_tables(self._h, der.ctypes.data_as(P), y.ctypes.data_as(P), dyl.ctypes.data_as(P))
+        self.der = der.reshape(5, 4, ny)  # der[j+2, n, iy] = der(iy, n, j)
+        self.y = y
+        self.dyl = dyl
+
+    def close(self):
+        if self._h:
+            lib().hst_gpu_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = lib().hst_gpu_last_error(self._h)
+            raise HstError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+    # ---- fields
+    def upload(self, field: int, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.complex128)
+        if a.shape != self.shape:
+            raise ValueError(f"field shape {a.shape}, expected {self.shape}")
+        self._check(lib().hst_gpu_upload(self._h, field, a.ctypes.data_as(ct.POINTER(ct.c_double))), "upload")
+
+    def download(self, field: int) -> np.ndarray:
+        a = np.empty(self.shape, np.complex128)
+        self._check(lib().hst_gpu_download(self._h, field, a.ctypes.data_as(ct.POINTER(ct.c_double))), "download")
+        return a
+
+    def set_velocity(self, V: np.ndarray):
+        """V: (3, nx+1, 2nz+1, ny+4) u, v, w; ghost rows are refilled at self.time."""
+        for c in range(3):
+            self.upload(c, V[c])
+            self.fill_ghosts(c)
+
+    def velocity(self) -> np.ndarray:
+        return np.stack([self.download(c) for c in range(3)])
+
+    def set_tables(self, der=None, y=None, dyl=None):
+        P = ct.POINTER(ct.c_double)
+        args = []
+        for a, n in ((der, 20 * self.ny), (y, self.ny + 4), (dyl, self.ny)):
+            if a is None:
+                args.append(None)
+            else:
+                a = np.ascontiguousarray(a, np.float64).ravel()
+                assert a.size == n
+                args.append(a)
+        self._check(lib().hst_gpu_set_tables(self._h, *[a.ctypes.data_as(P) if a is not None else None for a in args]),
+                    "set_tables")
+        self._tables()
+
+    # ---- the path
+    def timestep(self, deltat: float | None = None) -> float:
+        dt = self.deltat if deltat is None else float(deltat)
+        t = ct.c_double(self.time)
+        c = ct.c_double(0.0)
+        self._check(lib().hst_gpu_timestep(self._h, ct.byref(t), dt, ct.byref(c)), "timestep")
+        self.time = t.value
+        self.cfl = c.value
+        return self.cfl
+
+    def timesteps(self, n: int, deltat: float | None = None):
+        dt = self.deltat if deltat is None else float(deltat)
+        t = ct.c_double(self.time)
+        self._check(lib().hst_gpu_timesteps(self._h, int(n), ct.byref(t), dt), "timesteps")
+        self.time = t.value
+
+    def line_solve(self, kind, lam, src, dst, shift=None, time=None):
+        t = self.time if time is None else float(time)
+        if shift is None:
+            rc = lib().hst_gpu_line_solve(self._h, kind, float(lam), src, dst, 0, 0.0, 0.0, t)
+        else:
+            rc = lib().hst_gpu_line_solve(self._h, kind, float(lam), src, dst, 1, float(shift[0]), float(shift[1]), t)
+        self._check(rc, "line_solve")
+
+    def fill_ghosts(self, field, sx=None, sz=None):
+        if sx is None:
+            self._check(lib().hst_gpu_fill_ghosts_at(self._h, field, self.time), "fill_ghosts")
+        else:
+            self._check(lib().hst_gpu_fill_ghosts(self._h, field, float(sx), float(sz)), "fill_ghosts")
+
+    def compute_cfl(self) -> float:
+        c = ct.c_double(0.0)
+        self._check(lib().hst_gpu_compute_cfl(self._h, ct.byref(c)), "compute_cfl")
+        self.cfl = c.value
+        return c.value
+
+    def sync(self):
+        self._check(lib().hst_gpu_sync(self._h), "sync")
+
+    def shear_shifts(self, t):
+        sx, sz = ct.c_double(), ct.c_double()
+        lib().hst_gpu_shear_shifts(self._h, float(t), ct.byref(sx), ct.byref(sz))
+        return sx.value, sz.value
+
+    def s2_of(self, t):
+        return lib().hst_gpu_s2_of(self._h, float(t))
+
+    def s2_integral(self, t1, t2):
+        return lib().hst_gpu_s2_integral(self._h, float(t1), float(t2))
+
+    KERNEL_CLASSES = ("zinv", "xprod", "zfwd", "column", "line_solve", "ghosts")
+
+    def set_profiling(self, on: bool):
+        self._check(lib().hst_gpu_set_profiling(self._h, int(bool(on))), "set_profiling")
+
+    def kernel_times(self) -> dict:
+        """{class: (total ms, launches)} since the last reset (waits for the stream)."""
+        n = len(self.KERNEL_CLASSES)
+        ms = (ct.c_double * n)()
+        cnt = (ct.c_longlong * n)()
+        self._check(lib().hst_gpu_kernel_times(self._h, ms, cnt), "kernel_times")
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def reset_kernel_times(self):
+        self._check(lib().hst_gpu_reset_kernel_times(self._h), "reset_kernel_times")
+
+    def upload_ptr(self, field: int, ptr: int):
+        """upload from a host address (e.g. pinned memory) holding one field"""
+        self._check(lib().hst_gpu_upload(self._h, field, ct.cast(ct.c_void_p(ptr), ct.POINTER(ct.c_double))), "upload")
+
+    def download_ptr(self, field: int, ptr: int):
+        self._check(lib().hst_gpu_download(self._h, field, ct.cast(ct.c_void_p(ptr), ct.POINTER(ct.c_double))),
+                    "download")
+
+    @property
+    def launches(self) -> int:
+        return int(lib().hst_gpu_launch_count(self._h))
+
+    @property
+    def stream(self) -> int:
+        return int(lib().hst_gpu_stream(self._h) or 0)
+
+
+def device_bytes(**deck) -> float:
+    cfg = dict(DECK_DEFAULTS)
+    cfg.update(deck)
+    p = Params()
+    p.nx, p.ny, p.nz = int(cfg["nx"]), int(cfg["ny"]), int(cfg["nz"])
+    p.alfa0, p.beta0, p.ly, p.re = cfg["alfa0"], cfg["beta0"], cfg["ly"], cfg["re"]
+    return float(lib().hst_gpu_device_bytes(ct.byref(p)))
+
+
+# ------------------------------------------------------ initial fields ----
+def uniform_from_key(seed, component, iy, iz, ix):
+    """The keyed uniform deviate of src/hst_initial.f90:139-159, vectorised."""
+    M = np.uint64(0xFFFFFFFF)
+    h = (np.int64(seed) + np.int64(2654435761) * np.asarray(component, np.int64)
+         + np.int64(2246822519) * np.asarray(iy, np.int64) + np.int64(3266489917) * np.asarray(iz, np.int64)
+         + np.int64(668265263) * np.asarray(ix, np.int64))
+    h = h.astype(np.uint64) & M
+    h = h ^ (h >> np.uint64(16))
+    h = (h * np.uint64(2146121005)) & M
+    h = h ^ (h >> np.uint64(13))
+    h = (h * np.uint64(2032289749)) & M
+    h = h ^ (h >> np.uint64(16))
+    return h.astype(np.float64) * (1.0 / 4294967296.0)
+
+
+def random_field(nx, ny, nz, alfa0, beta0, ly, y, seed=1, k0=4.0, energy=0.1, envelope="gauss", amplitude=1.0):
+    """A seeded divergence-free field: the curl of a keyed random vector
+    potential (src/hst_initial.f90:27-67,113-133: modes |m| <= ny/3 in y,
+    (0,0) column zero, the ix = 0 plane Hermitian).  envelope 'gauss' is
+    exp(-(k/k0)^2) on the potential, i.e. E(k) ~ k^4 exp(-2 (k/k0)^2); 'hst'
+    is the reference's (k/k0)^2 exp(1 - (k/k0)^2).  With energy set, the
+    field is rescaled so that <u_i u_i>/2 = energy (box mean, as
+    src/hst_stats.f90:257-269 reports it).  Returns (3, nx+1, 2nz+1, ny+4)."""
+    mmax = ny // 3
+    ix = np.arange(nx + 1)[:, None, None]
+    iz = np.arange(-nz, nz + 1)[None, :, None]
+    m = np.arange(-mmax, mmax + 1)[None, None, :]
+    kx = alfa0 * ix
+    kz = beta0 * iz
+    ky = 2.0 * PI * m / ly
+    k = np.sqrt(kx * kx + ky * ky + kz * kz)
+    q = k / k0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        env = np.exp(-q * q) if envelope == "gauss" else q * q * np.exp(1.0 - q * q)
+    env = np.where((k == 0.0) | (env < 1e-8), 0.0, env)
+    env = np.where((ix == 0) & (iz == 0), 0.0, env)
+    mirror = (ix == 0) & ((iz < 0) | ((iz == 0) & (m < 0)))
+    jz = np.where(mirror, -iz, iz)
+    jm = np.where(mirror, -m, m)
+    a = []
+    for c in range(1, 4):
+        r = uniform_from_key(seed, c, jm, jz, ix)
+        ph = 2.0 * PI * uniform_from_key(seed, c + 3, jm, jz, ix)
+        ac = r * np.exp(1j * ph)
+        a.append(np.where(mirror, np.conj(ac), ac) * amplitude * env)
+    I = 1j
+    u = [I * (ky * a[2] - kz * a[1]), I * (kz * a[0] - kx * a[2]), I * (kx * a[1] - ky * a[0])]
+    E = np.exp(I * ky[0, 0, :, None] * y[None, :])  # (nm, ny+4)
+    V = np.stack([np.einsum("xzm,my->xzy", uc, E) for uc in u])
+    if energy is not None:
+        e = box_energy(V, ly, y)
+        if e > 0:
+            V *= math.sqrt(energy / e)
+    return V
+
+
+def box_energy(V, ly, y):
+    """<u_i u_i>/2 box mean from the spectral field (Parseval, weights dyl)."""
+    ny = V.shape[-1] - 4
+    dyl = 0.5 * (y[3:ny + 3] - y[1:ny + 1])
+    w = np.full(V.shape[1], 2.0)
+    w[0] = 1.0
+    q = (np.abs(V[:, :, :, 2:ny + 2]) ** 2 * w[None, :, None, None] * dyl[None, None, None, :]).sum()
+    return 0.5 * q / ly

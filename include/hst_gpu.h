@@ -1,0 +1,167 @@
+/*
+ * hst_gpu.h -- the C ABI of the B200 (sm_100a) implementation of the hst
+ * RK3 (Rai-Moin) / Crank-Nicolson substep.
+ *
+ * It replaces, one GPU per process and the whole field resident on it, the
+ * bodies of these Fortran module procedures of
+ * davecats/homogenenousShearTurbulence (paths relative to that project):
+ *   hst_equations   timestep, buildrhs_prepare, buildrhs, shear_shift, linsolve
+ *                   (src/hst_equations.f90:45)
+ *   hst_linsolve    line_solve, KIND_* (src/hst_linsolve.f90:79-83, 147-153)
+ *   hst_transforms  transform_to_physical, build_products, products_to_spectral,
+ *                   compute_cfl (src/hst_transforms.f90:27)
+ *   hst_derivatives fill_ghosts, fill_ghosts_field, shear_shifts, s2_of,
+ *                   s2_integral (src/hst_derivatives.f90:25-26)
+ *   hst_fft         device_sync (src/hst_fft.f90:162)
+ * The Fortran side (the hst.in deck, the Dati.cart files, the time loop)
+ * stays as it is; INTEGRATION.md shows the ISO_C_BINDING interface block.
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative HST_E* class;
+ *     hst_gpu_last_error() holds the message.  The Fortran shim turns a
+ *     non-zero status into `error stop`, as the reference's check()
+ *     (src/hst_fft.f90:169-176) does.
+ *   - Fields are complex128 (interleaved re, im) in the reference layout of
+ *     one component of V: V(iy, iz, ix) with iy = -2..ny+1 fastest, then
+ *     iz = -nz..nz, then ix = 0..nx (src/hst_params.f90:10-14, 101).
+ *   - The context owns all device memory and one CUDA stream; host pointers
+ *     are borrowed for the duration of a call.  Work is queued
+ *     asynchronously; the host waits only in downloads, in the CFL read of
+ *     hst_gpu_timestep and in hst_gpu_sync.  One host thread per context.
+ */
+#ifndef HST_GPU_H
+#define HST_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HST_GPU_ABI_VERSION 1
+
+/* status classes */
+#define HST_OK 0
+#define HST_EARG (-1)    /* bad argument or unsupported size */
+#define HST_ENOMEM (-2)  /* device allocation refused */
+#define HST_ECUDA (-3)   /* CUDA runtime error */
+#define HST_EFINITE (-5) /* non-finite CFL (the field blew up) */
+
+/* field ids: the three components of V, the carried explicit terms and the
+ * right-hand sides (src/hst_params.f90:101-103) */
+#define HST_V1 0
+#define HST_V2 1
+#define HST_V3 2
+#define HST_OLD1 3
+#define HST_OLD2 4
+#define HST_RHS1 5
+#define HST_RHS2 6
+
+/* line-solve kinds, KIND_D2V .. KIND_DY (src/hst_linsolve.f90:83) */
+#define HST_KIND_D2V 1
+#define HST_KIND_ETA 2
+#define HST_KIND_POISSON 3
+#define HST_KIND_D0 4
+#define HST_KIND_DY 5
+
+/* What the context needs from the deck (src/hst_input.f90:132-137 and the
+ * derived quantities :205-215).  nxd, nzd <= 0: derived as the reference
+ * does (fft_fit).  ystretch: the y grid of src/hst_setup.f90:80-89. */
+typedef struct hst_gpu_params {
+  int nx, ny, nz;
+  int nxd, nzd;
+  double alfa0, beta0, ly, ystretch;
+  double re, S;
+  int linear, exact_shift;
+  double s2_mean, s2_amplitude, s2_period, s2_start;
+  double damp_kpar, damp_kperp, damp_rate, damp_edge, damp_norm, damp_angle;
+  int damp_hard, damp_mean, damp_follow;
+  int device; /* CUDA device ordinal */
+} hst_gpu_params;
+
+typedef struct hst_ctx hst_ctx;
+
+/* ---------------------------------------------------------------- context */
+/* Allocates the device state, builds the y grid, der, k2 and the damping
+ * table on the host exactly as allocate_fields / setup_derivatives /
+ * damping_setup do (src/hst_setup.f90:42-71, src/hst_derivatives.f90:30-56,
+ * src/hst_damping.f90:68-78), uploads them.  The fields start at zero. */
+int hst_gpu_create(const hst_gpu_params* p, hst_ctx** out);
+int hst_gpu_destroy(hst_ctx* ctx);
+const char* hst_gpu_last_error(const hst_ctx* ctx);
+/* Device bytes held by a context of these sizes (0 on bad sizes). */
+double hst_gpu_device_bytes(const hst_gpu_params* p);
+
+/* Replaces the derivative table der(0:ny-1, 0:3, -2:2) (Fortran order),
+ * the grid y(-2:ny+1) and dyl(0:ny-1) by the caller's (a Fortran driver
+ * passes its own module arrays, src/hst_params.f90:84-88).  Any pointer may
+ * be NULL to keep the context's. */
+int hst_gpu_set_tables(hst_ctx* ctx, const double* der, const double* y, const double* dyl);
+/* Reads back the context's tables (same layouts). */
+int hst_gpu_get_tables(const hst_ctx* ctx, double* der, double* y, double* dyl);
+
+/* ----------------------------------------------------------------- fields */
+/* replaces `!$omp target update to(V)` / `from(V)` (src/hst.f90:76,110,121,141) */
+int hst_gpu_upload(hst_ctx* ctx, int field, const double* host);
+int hst_gpu_download(hst_ctx* ctx, int field, double* host);
+
+/* ------------------------------------------------------------------- path */
+/* timestep() (src/hst_equations.f90:56-87): three substeps; *time is
+ * advanced as the reference advances it; *cfl receives the CFL number of
+ * the third substep (compute_cfl, src/hst_transforms.f90:163-179). */
+int hst_gpu_timestep(hst_ctx* ctx, double* time, double deltat, double* cfl);
+/* timestep() n times in a row without reading the CFL (the host does not
+ * wait); *time is advanced. */
+int hst_gpu_timesteps(hst_ctx* ctx, int n, double* time, double deltat);
+
+/* line_solve(sys, lambda, src, dst [, shift_x, shift_z])
+ * (src/hst_linsolve.f90:147-233): has_shift = 0 uses the displacements of
+ * `time` (shear_shifts, src/hst_derivatives.f90:123-128). */
+int hst_gpu_line_solve(hst_ctx* ctx, int sys, double lambda, int src, int dst, int has_shift, double shift_x,
+                       double shift_z, double time);
+/* fill_ghosts_field(field, shift_x, shift_z) (src/hst_derivatives.f90:149-157) */
+int hst_gpu_fill_ghosts(hst_ctx* ctx, int field, double shift_x, double shift_z);
+/* fill_ghosts(c) at `time` (src/hst_derivatives.f90:134-145) */
+int hst_gpu_fill_ghosts_at(hst_ctx* ctx, int field, double time);
+
+/* transform_to_physical() + compute_cfl() (src/hst_transforms.f90:74-83,
+ * 163-179): the CFL number of the current V. */
+int hst_gpu_compute_cfl(hst_ctx* ctx, double* cfl);
+
+/* device_sync() (src/hst_fft.f90:162) */
+int hst_gpu_sync(hst_ctx* ctx);
+
+/* ------------------------------------------------------ host-side scalars */
+/* shear_shifts, s2_of, s2_integral (src/hst_derivatives.f90:85-128) for the
+ * context's S and S2 law */
+int hst_gpu_shear_shifts(const hst_ctx* ctx, double t, double* shift_x, double* shift_z);
+double hst_gpu_s2_of(const hst_ctx* ctx, double t);
+double hst_gpu_s2_integral(const hst_ctx* ctx, double t1, double t2);
+
+/* Kernel classes of the accounting below */
+#define HST_KC_ZINV 0       /* z-inverse transform of V */
+#define HST_KC_XPROD 1      /* x transforms + products + CFL */
+#define HST_KC_ZFWD 2       /* z-forward transform of the products */
+#define HST_KC_COLUMN 3     /* the fused column kernel (right-hand sides, shift, solves, u, w) */
+#define HST_KC_LINE_SOLVE 4 /* hst_gpu_line_solve */
+#define HST_KC_GHOSTS 5     /* hst_gpu_fill_ghosts */
+#define HST_KC_N 6
+
+/* Per-kernel device time: with profiling on, every launch is bracketed by
+ * two CUDA events on the context's stream; hst_gpu_kernel_times waits for
+ * the stream and returns, per class, the summed milliseconds and the number
+ * of launches since the last reset (arrays of HST_KC_N; either may be NULL).
+ * These have no counterpart in the reference, whose per-phase timer
+ * (src/hst_timer.f90:35-53) synchronises the device instead. */
+int hst_gpu_set_profiling(hst_ctx* ctx, int on);
+int hst_gpu_kernel_times(hst_ctx* ctx, double* ms, long long* count);
+int hst_gpu_reset_kernel_times(hst_ctx* ctx);
+
+/* Kernel launches made since the context was created (for accounting). */
+long long hst_gpu_launch_count(const hst_ctx* ctx);
+
+/* The stream the context queues its work on (a cudaStream_t). */
+void* hst_gpu_stream(const hst_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,59 @@
+"""The C ABI library loads and exports every entry point include/*.h
+declares; host-only paths (size checks, error statuses) work without a GPU."""
+import ctypes as ct
+import pathlib
+import re
+
+import pytest
+
+from homogenenousshearturbulence_b200 import hst
+
+ROOT = pathlib.Path(__file__).resolve().parent.parent
+
+
+def declared_functions():
+    names = []
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names += re.findall(r"\b(hst_gpu_\w+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    L = hst.lib()
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_bad_sizes_are_rejected_without_a_device():
+    p = hst.Params()
+    p.nx, p.ny, p.nz = 15, 31, 15           # odd ny: unsupported, refused before any CUDA call
+    p.alfa0, p.beta0, p.ly, p.re = 1.0, 1.0, 2.0, 100.0
+    h = ct.c_void_p()
+    rc = hst.lib().hst_gpu_create(ct.byref(p), ct.byref(h))
+    assert rc == -1 and not h.value
+    assert hst.lib().hst_gpu_device_bytes(ct.byref(p)) == 0.0
+
+
+def test_device_bytes_of_the_benchmark_configs():
+    # 512^3 (config 3) must fit in one B200's 180 GB with room to spare
+    b3 = hst.device_bytes(nx=255, ny=512, nz=256, alfa0=1.0, beta0=1.0, ly=6.283185307179586)
+    assert 20e9 < b3 < 60e9
+    b1 = hst.device_bytes(nx=31, ny=64, nz=32, alfa0=1.0, beta0=1.0, ly=6.283185307179586)
+    assert b1 < 1e9
+
+
+def test_null_context_calls_fail_cleanly():
+    L = hst.lib()
+    assert L.hst_gpu_destroy(None) == -1
+    assert L.hst_gpu_sync(None) == -1
+    assert L.hst_gpu_upload(None, 0, None) == -1
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    monkeypatch.setattr(hst, "LIB_PATH", tmp_path / "absent.so")
+    monkeypatch.setattr(hst, "_lib", None)
+    with pytest.raises(hst.HstError):
+        hst.lib()
