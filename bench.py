@@ -63,9 +63,12 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def alg_bytes(deck, nxd, nzd):
+def alg_bytes(deck, nxd, nzd, split):
     """Compulsory HBM bytes per launch of each kernel and per substep (FP64).
-    Ns = ny (2nz+1)(nx+1) spectral points per component, Nzx = ny nzd (nx+1)."""
+    Ns = ny (2nz+1)(nx+1) spectral points per component, Nzx = ny nzd (nx+1).
+    With the column stage split, `rhs` streams V, Q, old in and old, rhs out
+    (15 Ns) and `column` reads rhs and writes V (5 Ns; 9 Ns with exact_shift,
+    which re-reads and rewrites old); fused, `column` moves 16 Ns."""
     nx, ny, nz = deck["nx"], deck["ny"], deck["nz"]
     Ns = ny * (2 * nz + 1) * (nx + 1)
     Nzx = ny * nzd * (nx + 1)
@@ -74,7 +77,8 @@ def alg_bytes(deck, nxd, nzd):
         "zinv": b * (3 * Ns + 3 * Nzx),
         "xprod": b * (3 * Nzx + 6 * Nzx),
         "zfwd": b * (6 * Nzx + 6 * Ns),
-        "column": b * (16 * Ns),
+        "rhs": b * (15 * Ns),
+        "column": b * ((9 if deck.get("exact_shift") else 5) * Ns if split else 16 * Ns),
     }
     return k, b * (25 * Ns + 18 * Nzx), Ns, Nzx
 
@@ -282,7 +286,7 @@ def main():
                "d2h_bytes_per_step": 3 * nbytes + 8, "steps": ke}
 
     if rank == 0:
-        per_kernel, b_sub, Ns, Nzx = alg_bytes(deck, s.nxd, s.nzd)
+        per_kernel, b_sub, Ns, Nzx = alg_bytes(deck, s.nxd, s.nzd, ktimes.get("rhs", (0, 0))[1] > 0)
         peak, peak_kind = peaks()
         kt = {k: v for k, v in ktimes.items() if v[1] > 0}
         top = max(kt, key=lambda k: kt[k][0])

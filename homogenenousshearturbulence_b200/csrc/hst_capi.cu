@@ -141,6 +141,9 @@ struct hst_ctx {
   std::string err;
   long long launches;
   int device;
+  // the column stage as two kernels (right-hand sides streamed row by row,
+  // then the solves) or one; HST_COLUMN_FUSED=1 selects the single kernel
+  bool column_split;
   // per-kernel-class CUDA-event accounting (hst_gpu_set_profiling)
   bool prof_on;
   std::vector<cudaEvent_t> ev;
@@ -277,14 +280,15 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
   g.rows = p.ny + 4;
   g.ncol = g.nxB * g.nzT;
   g.nf = (long)g.ncol * g.rows;
-  // line-solve group: P lanes of m rows; prefer m >= 16, accept m >= 4
+  // line-solve group: P lanes of m rows; the widest group with m >= 8
+  // (measured best at 384^2 x 256), else m >= 4
   int P = 0;
   const char* env = std::getenv("HST_LINE_LANES");
   if (env) {
     int e = std::atoi(env);
     if (e >= 2 && e <= 32 && (e & (e - 1)) == 0 && p.ny % e == 0 && p.ny / e >= 4) P = e;
   }
-  for (int mmin : {16, 8, 4}) {
+  for (int mmin : {8, 4}) {
     if (P) break;
     for (int c = 32; c >= 2; c >>= 1)
       if (p.ny % c == 0 && p.ny / c >= mmin) {
@@ -307,9 +311,10 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
       break;
     }
   }
-  g.ppt = 8;
-  if (2 * g.nxd * 6 / 8 > 1024 || g.Ty * g.nzd / 8 > 1024) {
-    why = "transform length too large for this build";
+  g.ppt = 16;
+  if (!hst::fft_length_ok(2 * g.nxd) || !hst::fft_length_ok(g.nzd) || g.Ty * g.nzd > 32 * 256 ||
+      6 * 2 * g.nxd > 32 * 320) {
+    why = "transform length not supported (2 nxd <= 1536, radices 2, 3, 4, 6, 8, 12, 16, 24)";
     return HST_EARG;
   }
   return HST_OK;
@@ -328,6 +333,17 @@ extern "C" double hst_gpu_device_bytes(const hst_gpu_params* p) {
   return dev_bytes(g);
 }
 
+// der in the slab-major order of hst::SlabDer
+static std::vector<double> slab_major(const std::vector<double>& der, int ny, int P, int m) {
+  std::vector<double> o((size_t)20 * ny);
+  for (int n = 0; n < 4; ++n)
+    for (int j = 0; j < 5; ++j)
+      for (int i = 0; i < m; ++i)
+        for (int s = 0; s < P; ++s)
+          o[((size_t)(n * 5 + j) * m + i) * P + s] = der[(size_t)(s * m + i) + (size_t)ny * (n + 4 * j)];
+  return o;
+}
+
 static std::vector<double2> twiddles(int n) {
   std::vector<double2> t(n);
   for (int k = 0; k < n; ++k) {
@@ -341,7 +357,7 @@ static void free_device(hst_ctx* c) {
   DeviceState& d = c->d;
   for (int i = 0; i < 7; ++i)
     if (d.F[i]) cudaFree(d.F[i]);
-  void* ps[] = {d.Z, d.Pp, d.Q, d.der, d.y, d.dyl, d.gdamp, d.twx, d.twz, d.cfl};
+  void* ps[] = {d.Z, d.Pp, d.Q, d.der, d.derS, d.y, d.dyl, d.gdamp, d.twx, d.twz, d.cfl};
   for (void* q : ps)
     if (q) cudaFree(q);
   std::memset(&d, 0, sizeof d);
@@ -354,6 +370,10 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   if (!ctx) return HST_ENOMEM;
   ctx->p = *pin;
   ctx->launches = 0;
+  {
+    const char* e = std::getenv("HST_COLUMN_FUSED");
+    ctx->column_split = !(e && std::atoi(e) == 1);
+  }
   ctx->prof_on = false;
   for (int k = 0; k < HST_KC_N; ++k) {
     ctx->prof_ms[k] = 0.0;
@@ -418,12 +438,15 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   ok = ok && alloc((void**)&d.Pp, sizeof(double2) * 6 * (size_t)g.nzd * g.ny * g.nxB);
   ok = ok && alloc((void**)&d.Q, sizeof(double2) * 6 * (size_t)g.ncol * g.ny);
   ok = ok && alloc((void**)&d.der, sizeof(double) * 20 * (size_t)ny);
+  ok = ok && alloc((void**)&d.derS, sizeof(double) * 20 * (size_t)ny);
   ok = ok && alloc((void**)&d.y, sizeof(double) * (ny + 4));
   ok = ok && alloc((void**)&d.dyl, sizeof(double) * ny);
   ok = ok && alloc((void**)&d.gdamp, sizeof(double) * g.ncol);
   ok = ok && alloc((void**)&d.twx, sizeof(double2) * 2 * g.nxd);
   ok = ok && alloc((void**)&d.twz, sizeof(double2) * g.nzd);
-  ok = ok && alloc((void**)&d.cfl, sizeof(unsigned long long));
+  // two words: the CFL maximum and the bounded-wait error flag
+  ok = ok && alloc((void**)&d.cfl, 2 * sizeof(unsigned long long));
+  if (ok) d.err = reinterpret_cast<int*>(d.cfl + 1);
   if (!ok) {
     free_device(ctx);
     std::fprintf(stderr, "hst_gpu_create: device allocation of %.2f GB refused\n", dev_bytes(g) / 1e9);
@@ -432,20 +455,26 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   }
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMallocHost((void**)&ctx->h_gdamp, sizeof(double) * g.ncol) != cudaSuccess ||
-      cudaMallocHost((void**)&ctx->h_cfl, sizeof(unsigned long long)) != cudaSuccess) {
+      cudaMallocHost((void**)&ctx->h_cfl, 2 * sizeof(unsigned long long)) != cudaSuccess) {
     free_device(ctx);
     delete ctx;
     return HST_ECUDA;
   }
   for (int i = 0; i < 7; ++i) cudaMemsetAsync(d.F[i], 0, sizeof(double2) * g.nf, ctx->stream);
+  cudaMemsetAsync(d.cfl, 0, 2 * sizeof(unsigned long long), ctx->stream);
   auto tx = twiddles(2 * g.nxd), tz = twiddles(g.nzd);
   cudaMemcpy(d.der, ctx->der.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice);
+  {
+    auto ds = slab_major(ctx->der, ny, g.P, g.m);
+    cudaMemcpy(d.derS, ds.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice);
+  }
   cudaMemcpy(d.y, ctx->y.data(), sizeof(double) * (ny + 4), cudaMemcpyHostToDevice);
   cudaMemcpy(d.dyl, ctx->dyl.data(), sizeof(double) * ny, cudaMemcpyHostToDevice);
   cudaMemcpy(d.gdamp, ctx->gdamp.data(), sizeof(double) * g.ncol, cudaMemcpyHostToDevice);
   cudaMemcpy(d.twx, tx.data(), sizeof(double2) * tx.size(), cudaMemcpyHostToDevice);
   cudaMemcpy(d.twz, tz.data(), sizeof(double2) * tz.size(), cudaMemcpyHostToDevice);
-  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaError_t e = hst::set_fft_constants();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
     std::fprintf(stderr, "hst_gpu_create: %s\n", cudaGetErrorString(e));
@@ -480,7 +509,9 @@ extern "C" int hst_gpu_set_tables(hst_ctx* ctx, const double* der, const double*
   CK(cudaSetDevice(ctx->device));
   if (der) {
     std::memcpy(ctx->der.data(), der, sizeof(double) * 20 * ny);
-    CK(cudaMemcpyAsync(ctx->d.der, ctx->der.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpy(ctx->d.der, ctx->der.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice));
+    auto ds = slab_major(ctx->der, ny, ctx->g.P, ctx->g.m);
+    CK(cudaMemcpy(ctx->d.derS, ds.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice));
   }
   if (y) {
     std::memcpy(ctx->y.data(), y, sizeof(double) * (ny + 4));
@@ -562,8 +593,12 @@ extern "C" int hst_gpu_line_solve(hst_ctx* ctx, int sys, double lambda, int src,
 }
 
 static int read_cfl(hst_ctx* ctx, double* cfl) {
-  CK(cudaMemcpyAsync(ctx->h_cfl, ctx->d.cfl, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->h_cfl, ctx->d.cfl, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->h_cfl[1] != 0) {
+    CK(cudaMemsetAsync(ctx->d.err, 0, sizeof(int), ctx->stream));
+    return fail(ctx, HST_ETIMEOUT, "a kernel's bounded wait for its TMA copies ran out; the step is invalid");
+  }
   unsigned long long b = *ctx->h_cfl;
   double v;
   std::memcpy(&v, &b, sizeof v);
@@ -617,8 +652,15 @@ static int queue_timestep(hst_ctx* ctx, double* time, double deltat) {
     sc.dgz = s2_integral(p, t, t + dt_sub);
     shear_shifts(ctx, t, &sc.sx_t, &sc.sz_t);
     shear_shifts(ctx, t + dt_sub, &sc.sx_n, &sc.sz_n);
-    CK(timed(ctx, HST_KC_COLUMN,
-             [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, ctx->stream); }));
+    if (ctx->column_split) {
+      CK(timed(ctx, HST_KC_RHS,
+               [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, 1, ctx->stream); }));
+      CK(timed(ctx, HST_KC_COLUMN,
+               [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, 2, ctx->stream); }));
+    } else {
+      CK(timed(ctx, HST_KC_COLUMN,
+               [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, 0, ctx->stream); }));
+    }
     *time = t + dt_sub;
   }
   return HST_OK;

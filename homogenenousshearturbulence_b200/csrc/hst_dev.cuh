@@ -43,6 +43,41 @@ __device__ __forceinline__ cxd shfl_c(unsigned mask, cxd v, int src, int width) 
   return mkc(__shfl_sync(mask, v.x, src, width), __shfl_sync(mask, v.y, src, width));
 }
 
+// ------------------------------------------- TMA bulk copies, mbarriers ----
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// 1-D bulk copy global -> this CTA's shared memory, completion counted on
+// bar (16-byte aligned addresses, size a multiple of 16; no multicast)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for the phase `parity` of bar to complete, at most `limit` polls;
+// false when the limit ran out (the caller records an error and returns).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int limit) {
+  for (int i = 0; i < limit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
 // line-solve kinds (src/hst_linsolve.f90:83)
 enum { K_D2V = 1, K_ETA = 2, K_POISSON = 3, K_D0 = 4, K_DY = 5 };
 
@@ -52,40 +87,38 @@ __device__ __forceinline__ double derv(const double* __restrict__ der, int ny, i
   return __ldg(der + iy + ny * (n + 4 * (j + 2)));
 }
 
-// The five band entries of row iy of system `sys` before the wrap phase:
-// coef, src/hst_linsolve.f90:236-252.
-__device__ __forceinline__ void row_coefs(int sys, double lambda, double ni, double kk, const double* __restrict__ der,
-                                          int ny, int iy, double a[5]) {
+// The same table in slab-major order for a line-solve group of P lanes and
+// m rows per lane: derS[((n*5 + j)*m + i)*P + s] = der(s*m + i, n, j - 2),
+// so that the P lanes reading row i of their own slabs read consecutive
+// addresses.
+struct SlabDer {
+  const double* __restrict__ p;
+  int m, P;
+  __device__ __forceinline__ double operator()(int s, int i, int n, int j) const {
+    return __ldg(p + ((size_t)((n * 5 + j) * m + i)) * P + s);
+  }
+};
+
+// The five band entries of row i of slab s of system `sys` before the wrap
+// phase: coef, src/hst_linsolve.f90:236-252.
+__device__ __forceinline__ void row_coefs(int sys, double lambda, double ni, double kk, const SlabDer& D, int s, int i,
+                                          double a[5]) {
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
-    double d0 = derv(der, ny, iy, 0, j - 2);
+    double d0 = D(s, i, 0, j);
     if (sys == K_D2V) {
-      double d2 = derv(der, ny, iy, 2, j - 2), d4 = derv(der, ny, iy, 3, j - 2);
+      double d2 = D(s, i, 2, j), d4 = D(s, i, 3, j);
       a[j] = lambda * (d2 - kk * d0) - ni * (d4 - 2.0 * kk * d2 + kk * kk * d0);
     } else if (sys == K_ETA) {
-      double d2 = derv(der, ny, iy, 2, j - 2);
+      double d2 = D(s, i, 2, j);
       a[j] = lambda * d0 - ni * (d2 - kk * d0);
     } else if (sys == K_POISSON) {
-      double d2 = derv(der, ny, iy, 2, j - 2);
+      double d2 = D(s, i, 2, j);
       a[j] = d2 - kk * d0;
     } else {
       a[j] = d0;
     }
   }
-}
-__device__ __forceinline__ double row_coef(int sys, double lambda, double ni, double kk, const double* __restrict__ der,
-                                           int ny, int iy, int j) {
-  double d0 = derv(der, ny, iy, 0, j);
-  if (sys == K_D2V) {
-    double d2 = derv(der, ny, iy, 2, j), d4 = derv(der, ny, iy, 3, j);
-    return lambda * (d2 - kk * d0) - ni * (d4 - 2.0 * kk * d2 + kk * kk * d0);
-  } else if (sys == K_ETA) {
-    double d2 = derv(der, ny, iy, 2, j);
-    return lambda * d0 - ni * (d2 - kk * d0);
-  } else if (sys == K_POISSON) {
-    return derv(der, ny, iy, 2, j) - kk * d0;
-  }
-  return d0;
 }
 
 // ------------------------------------------------ 2x2 block helpers ----
@@ -210,10 +243,9 @@ struct LineGeom {
 // fac: per-lane factor scratch, (m-2) x 4 x P doubles.
 // Rows of the right-hand side of KIND_DY must already hold D1 src.
 template <int P>
-__device__ void group_solve(int sys, double lambda, double ni, double kk, double theta, const double* __restrict__ der,
-                            int ny, const LineGeom& G, cxd* buf, double* fac, int s, unsigned gmask) {
+__device__ void group_solve(int sys, double lambda, double ni, double kk, double theta, const SlabDer& DS,
+                            const LineGeom& G, cxd* buf, double* fac, int s, unsigned gmask) {
   const int m = G.m, mi = m - 2, MS = G.MS;
-  const int r0 = s * m;
   cxd* sb = buf + s * MS;
   // ---- forward sweep of the slab interior (penta_forward)
   double u11 = 0, u12 = 0, p1 = 0, q1 = 0, u21 = 0, u22 = 0, p2 = 0, q2 = 0;
@@ -221,7 +253,7 @@ __device__ void group_solve(int sys, double lambda, double ni, double kk, double
   cxd x1 = mkc(0, 0), x2 = mkc(0, 0), sx0 = mkc(0, 0), sx1 = mkc(0, 0);
   for (int i = 0; i < mi; ++i) {
     double a[5];
-    row_coefs(sys, lambda, ni, kk, der, ny, r0 + i, a);
+    row_coefs(sys, lambda, ni, kk, DS, s, i, a);
     double p = 0, q = 0;
     if (i == 0) {
       p = a[0];
@@ -294,14 +326,12 @@ __device__ void group_solve(int sys, double lambda, double ni, double kk, double
   const double T3 = shfl_d(gmask, R3, t, P), T4 = shfl_d(gmask, R4, t, P), T5 = shfl_d(gmask, R5, t, P),
                T6 = shfl_d(gmask, R6, t, P), T9 = shfl_d(gmask, R9, t, P), T10 = shfl_d(gmask, R10, t, P),
                T11 = shfl_d(gmask, R11, t, P), T12 = shfl_d(gmask, R12, t, P);
-  // the two border rows of the slab (global rows ga, ga+1)
-  const int ga = r0 + mi;
-  const double c1m4 = row_coef(sys, lambda, ni, kk, der, ny, ga, -2), c1m3 = row_coef(sys, lambda, ni, kk, der, ny, ga, -1);
-  const double d11 = row_coef(sys, lambda, ni, kk, der, ny, ga, 0), d12 = row_coef(sys, lambda, ni, kk, der, ny, ga, 1);
-  const double c10 = row_coef(sys, lambda, ni, kk, der, ny, ga, 2);
-  const double c2m3 = row_coef(sys, lambda, ni, kk, der, ny, ga + 1, -2), d21 = row_coef(sys, lambda, ni, kk, der, ny, ga + 1, -1);
-  const double d22 = row_coef(sys, lambda, ni, kk, der, ny, ga + 1, 0), c20 = row_coef(sys, lambda, ni, kk, der, ny, ga + 1, 1);
-  const double c21 = row_coef(sys, lambda, ni, kk, der, ny, ga + 1, 2);
+  // the two border rows of the slab (its rows mi, mi+1)
+  double ab1[5], ab2[5];
+  row_coefs(sys, lambda, ni, kk, DS, s, mi, ab1);
+  row_coefs(sys, lambda, ni, kk, DS, s, mi + 1, ab2);
+  const double c1m4 = ab1[0], c1m3 = ab1[1], d11 = ab1[2], d12 = ab1[3], c10 = ab1[4];
+  const double c2m3 = ab2[0], d21 = ab2[1], d22 = ab2[2], c20 = ab2[3], c21 = ab2[4];
   // phases: ph = exp(-i theta) across the box edge; mu = ph^(1/P)
   const cxd ph = cexpi(-theta);
   const cxd mu = cexpi(-(theta / (double)P));

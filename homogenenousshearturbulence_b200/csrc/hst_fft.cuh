@@ -1,13 +1,21 @@
-// Shared-memory Stockham FFT for the 3/2-dealiased x and z transforms.
+// Stockham FFTs for the 3/2-dealiased x and z transforms.
 //
-// Several lines of length N (N = 2^a 3^b) sit in shared memory; all threads
-// of the block cooperate on every radix stage: a thread loads the R inputs
-// of its butterflies into registers, the block synchronises, and the
-// outputs overwrite the same buffer (in place, so one copy of the lines is
-// enough).  Twiddles come from a table W[e] = exp(-2 pi i e / N) computed on
-// the host in extended precision.  Unnormalised in both directions, like
-// the reference's FFTW / cuFFT plans (src/hst_fft.f90:98-121): sign -1 is
-// the forward transform exp(-2 pi i j k / N), sign +1 the backward one.
+// A block transforms nl lines of length N = 2^a 3^b.  Each radix-R stage
+// is one pass: a thread gathers the R inputs of its butterflies into
+// registers, applies the stage twiddles, computes a radix-R DFT in
+// registers (R up to 24, built from radix-2/3/4 pieces), and scatters the
+// outputs.  The first stage reads through a caller's loader (global memory,
+// or a function of other lines) and the last stage writes through a
+// caller's storer, so only the exchanges between stages go through shared
+// memory: N = 384 is two stages (16 x 24) with one shared exchange, N = 768
+// three stages.  Threads are mapped line-fastest so that global accesses of
+// consecutive threads touch consecutive lines (the y rows, contiguous in
+// memory); shared lines have an odd stride against bank conflicts.
+// Stage twiddles come from W[e] = exp(-2 pi i e / N) in global memory, the
+// twiddles inside a register DFT from a 48-entry table in constant memory
+// (all threads read the same entry).  Both tables are computed on the host
+// in extended precision.  Unnormalised both ways, like the reference's FFTW
+// and cuFFT plans (src/hst_fft.f90:98-121): S = -1 forward, S = +1 backward.
 #pragma once
 #include "hst_dev.cuh"
 
@@ -15,93 +23,265 @@ namespace hst {
 
 #define HST_SQRT3_2 0.86602540378443864676
 
-template <int R>
-__device__ __forceinline__ void butterfly(cxd* v, int sign) {
-  if (R == 2) {
+// exp(-2 pi i k / 48), k = 0..47 (set per device by set_fft_constants;
+// this header is included by one translation unit only)
+__constant__ double2 c_w48[48];
+
+template <int R, int S>
+struct DFT;
+
+template <int S>
+struct DFT<2, S> {
+  static __device__ __forceinline__ void run(cxd* v) {
     cxd a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
-  } else if (R == 4) {
+  }
+};
+template <int S>
+struct DFT<4, S> {
+  static __device__ __forceinline__ void run(cxd* v) {
     cxd a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]), a2 = cadd(v[1], v[3]), a3 = csub(v[1], v[3]);
-    cxd a3r = sign < 0 ? mkc(a3.y, -a3.x) : mkc(-a3.y, a3.x);
+    cxd a3r = S < 0 ? mkc(a3.y, -a3.x) : mkc(-a3.y, a3.x);
     v[0] = cadd(a0, a2);
     v[2] = csub(a0, a2);
     v[1] = cadd(a1, a3r);
     v[3] = csub(a1, a3r);
-  } else if (R == 3) {
+  }
+};
+template <int S>
+struct DFT<3, S> {
+  static __device__ __forceinline__ void run(cxd* v) {
     cxd t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
     cxd m = mkc(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-    // (-i sign') sqrt(3)/2 t2, forward: -i
-    cxd r = sign < 0 ? mkc(HST_SQRT3_2 * t2.y, -HST_SQRT3_2 * t2.x) : mkc(-HST_SQRT3_2 * t2.y, HST_SQRT3_2 * t2.x);
+    cxd r = S < 0 ? mkc(HST_SQRT3_2 * t2.y, -HST_SQRT3_2 * t2.x) : mkc(-HST_SQRT3_2 * t2.y, HST_SQRT3_2 * t2.x);
     v[0] = cadd(v[0], t1);
     v[1] = cadd(m, r);
     v[2] = csub(m, r);
   }
+};
+// R = A B: B DFTs of size A on the elements b + B a, the twiddles
+// W_R^(b ka), A DFTs of size B; output k = ka + A kb.
+template <int A, int B, int S>
+__device__ __forceinline__ void dft_ab(cxd* v) {
+  cxd o[A * B];
+#pragma unroll
+  for (int b = 0; b < B; ++b) {
+    cxd t[A];
+#pragma unroll
+    for (int a = 0; a < A; ++a) t[a] = v[b + B * a];
+    DFT<A, S>::run(t);
+#pragma unroll
+    for (int ka = 0; ka < A; ++ka) {
+      if (b * ka == 0) {
+        v[b + B * ka] = t[ka];
+      } else {
+        cxd w = c_w48[(b * ka * (48 / (A * B))) % 48];
+        if (S > 0) w.y = -w.y;
+        v[b + B * ka] = cmul(t[ka], w);
+      }
+    }
+  }
+#pragma unroll
+  for (int ka = 0; ka < A; ++ka) {
+    cxd t[B];
+#pragma unroll
+    for (int b = 0; b < B; ++b) t[b] = v[b + B * ka];
+    DFT<B, S>::run(t);
+#pragma unroll
+    for (int kb = 0; kb < B; ++kb) o[ka + A * kb] = t[kb];
+  }
+#pragma unroll
+  for (int k = 0; k < A * B; ++k) v[k] = o[k];
+}
+template <int S>
+struct DFT<6, S> {
+  static __device__ __forceinline__ void run(cxd* v) { dft_ab<3, 2, S>(v); }
+};
+template <int S>
+struct DFT<8, S> {
+  static __device__ __forceinline__ void run(cxd* v) { dft_ab<4, 2, S>(v); }
+};
+template <int S>
+struct DFT<12, S> {
+  static __device__ __forceinline__ void run(cxd* v) { dft_ab<4, 3, S>(v); }
+};
+template <int S>
+struct DFT<16, S> {
+  static __device__ __forceinline__ void run(cxd* v) { dft_ab<4, 4, S>(v); }
+};
+template <int S>
+struct DFT<24, S> {
+  static __device__ __forceinline__ void run(cxd* v) { dft_ab<8, 3, S>(v); }
+};
+
+// The runtime radix plan of N: radix-16 stages while more than 24 is left,
+// then the rest in one stage (2, 3, 4, 6, 8, 12, 16 or 24).
+struct FftPlan {
+  int n;
+  int r[4];
+};
+__host__ __device__ inline FftPlan make_plan(int N) {
+  FftPlan p;
+  p.n = 0;
+  int m = N;
+  while (m > 24 && m % 16 == 0 && p.n < 3) {
+    p.r[p.n++] = 16;
+    m /= 16;
+  }
+  if (m > 1) p.r[p.n++] = m;
+  return p;
+}
+__host__ inline bool plan_ok(int N) {
+  FftPlan p = make_plan(N);
+  int prod = 1;
+  for (int i = 0; i < p.n; ++i) {
+    int r = p.r[i];
+    if (!(r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 12 || r == 16 || r == 24)) return false;
+    prod *= r;
+  }
+  return prod == N;
 }
 
-// One radix-R Stockham stage on nl lines (line stride LS) of length N, where
-// Ns is the product of the radices already applied.  MAXB bounds the
-// butterflies per thread: nl*N/R <= MAXB*blockDim.x.
-template <int R, int MAXB>
-__device__ __forceinline__ void fft_stage(cxd* data, int N, int nl, int LS, int Ns, const cxd* __restrict__ tw,
-                                          int sign) {
+// Shared-memory line access (line stride LS)
+struct ShLines {
+  cxd* p;
+  int LS;
+  __device__ __forceinline__ cxd operator()(int l, int i) const { return p[l * LS + i]; }
+  __device__ __forceinline__ void operator()(int l, int i, cxd v) const { p[l * LS + i] = v; }
+};
+
+// One radix-R stage.  Butterfly b of the block: line l = b % nl, index
+// j = b / nl.  Inputs ld(l, j + r N/R), outputs st(l, (j/Ns) Ns R + j%Ns + r Ns).
+// SYNC: the stage reads and writes the same shared lines (all reads, then
+// a barrier, then all writes).
+template <int R, int S, int PPT, bool SYNC, typename LD, typename ST>
+__device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const cxd* __restrict__ tw, const LD& ld,
+                                             const ST& st) {
+  constexpr int MAXB = (PPT + R - 1) / R;
   const int nb = N / R;
   const int total = nb * nl;
   const int tstride = N / (Ns * R);
   cxd v[MAXB][R];
-  int dst[MAXB];
+  int lj[MAXB];
 #pragma unroll
   for (int k = 0; k < MAXB; ++k) {
     int b = threadIdx.x + k * blockDim.x;
-    dst[k] = -1;
+    lj[k] = -1;
     if (b < total) {
-      int line = b / nb, j = b - line * nb;
-      const cxd* L = data + line * LS;
+      int l = b % nl, j = b / nl;
       int kk = j % Ns;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        cxd x = L[j + r * nb];
-        if (r > 0) {
+        cxd x = ld(l, j + r * nb);
+        if (r > 0 && kk > 0) {
           cxd w = __ldg(tw + kk * r * tstride);
-          if (sign > 0) w.y = -w.y;
+          if (S > 0) w.y = -w.y;
           x = cmul(x, w);
         }
         v[k][r] = x;
       }
-      butterfly<R>(v[k], sign);
-      dst[k] = line * LS + (j / Ns) * Ns * R + kk;
+      DFT<R, S>::run(v[k]);
+      lj[k] = b;
     }
   }
-  __syncthreads();
+  if (SYNC) __syncthreads();
 #pragma unroll
   for (int k = 0; k < MAXB; ++k) {
-    if (dst[k] >= 0) {
+    if (lj[k] >= 0) {
+      int l = lj[k] % nl, j = lj[k] / nl;
+      int kk = j % Ns;
+      int base = (j / Ns) * Ns * R + kk;
 #pragma unroll
-      for (int r = 0; r < R; ++r) data[dst[k] + r * Ns] = v[k][r];
+      for (int r = 0; r < R; ++r) st(l, base + r * Ns, v[k][r]);
     }
   }
-  __syncthreads();
 }
 
-// The radix plan of N = 4^a 2^b 3^c (b, c <= 1): radix-4 stages, then one
-// radix-2, then one radix-3.  PPT bounds the points per thread.
-template <int PPT>
-__device__ void fft_lines(cxd* data, int N, int nl, int LS, const cxd* __restrict__ tw, int sign) {
-  int n = N, Ns = 1;
-  while (n % 4 == 0) {
-    fft_stage<4, (PPT + 3) / 4>(data, N, nl, LS, Ns, tw, sign);
-    n /= 4;
-    Ns *= 4;
+template <int S, int PPT, bool SYNC, typename LD, typename ST>
+__device__ __forceinline__ void fft_stage_r(int R, int N, int nl, int Ns, const cxd* __restrict__ tw, const LD& ld,
+                                            const ST& st) {
+  switch (R) {
+    case 2: fft_stage_io<2, S, PPT, SYNC>(N, nl, Ns, tw, ld, st); break;
+    case 3: fft_stage_io<3, S, PPT, SYNC>(N, nl, Ns, tw, ld, st); break;
+    case 4: fft_stage_io<4, S, PPT, SYNC>(N, nl, Ns, tw, ld, st); break;
+    case 6: fft_stage_io<6, S, PPT, SYNC>(N, nl, Ns, tw, ld, st); break;
+    case 8: fft_stage_io<8, S, PPT, SYNC>(N, nl, Ns, tw, ld, st); break;
+    case 12: fft_stage_io<12, S, PPT, SYNC>(N, nl, Ns, tw, ld, st); break;
+    case 16: fft_stage_io<16, S, PPT, SYNC>(N, nl, Ns, tw, ld, st); break;
+    case 24: fft_stage_io<24, S, PPT, SYNC>(N, nl, Ns, tw, ld, st); break;
+    default: break;
   }
-  if (n % 2 == 0) {
-    fft_stage<2, (PPT + 1) / 2>(data, N, nl, LS, Ns, tw, sign);
-    n /= 2;
-    Ns *= 2;
+}
+
+// The whole transform of nl lines with the runtime plan: the first stage
+// reads through src, the last writes through dst, the stages between
+// exchange through `sh` (nl lines of stride N+1).  SRC_SH / DST_SH: src
+// reads, dst writes the same shared buffer (the stage then synchronises
+// between its reads and its writes).  Requires nl N <= PPT blockDim.x.
+template <int S, int PPT, bool SRC_SH, bool DST_SH, typename LD, typename ST>
+__device__ void fft_global(int N, int nl, const cxd* __restrict__ tw, cxd* sh, const LD& src, const ST& dst) {
+  const FftPlan P = make_plan(N);
+  const ShLines L = {sh, N + 1};
+  int Ns = 1;
+  if (P.n == 1) {
+    fft_stage_r<S, PPT, SRC_SH && DST_SH>(P.r[0], N, nl, Ns, tw, src, dst);
+    return;
   }
-  if (n % 3 == 0) {
-    fft_stage<3, (PPT + 2) / 3>(data, N, nl, LS, Ns, tw, sign);
-    n /= 3;
-    Ns *= 3;
+  fft_stage_r<S, PPT, SRC_SH>(P.r[0], N, nl, Ns, tw, src, L);
+  Ns *= P.r[0];
+  __syncthreads();
+  for (int s = 1; s + 1 < P.n; ++s) {
+    fft_stage_r<S, PPT, true>(P.r[s], N, nl, Ns, tw, L, L);
+    Ns *= P.r[s];
+    __syncthreads();
+  }
+  fft_stage_r<S, PPT, DST_SH>(P.r[P.n - 1], N, nl, Ns, tw, L, dst);
+}
+
+// Compile-time plans of the lengths the configurations use (the 3/2-padded
+// sizes 2^a 3 from 12 to 1536), so that each kernel instantiates only the
+// radices it runs.
+template <int N>
+struct Plan {
+  static constexpr int n = 0, r0 = 1, r1 = 1, r2 = 1;
+};
+template <> struct Plan<12> { static constexpr int n = 1, r0 = 12, r1 = 1, r2 = 1; };
+template <> struct Plan<24> { static constexpr int n = 1, r0 = 24, r1 = 1, r2 = 1; };
+template <> struct Plan<48> { static constexpr int n = 2, r0 = 16, r1 = 3, r2 = 1; };
+template <> struct Plan<96> { static constexpr int n = 2, r0 = 16, r1 = 6, r2 = 1; };
+template <> struct Plan<192> { static constexpr int n = 2, r0 = 16, r1 = 12, r2 = 1; };
+template <> struct Plan<384> { static constexpr int n = 2, r0 = 16, r1 = 24, r2 = 1; };
+template <> struct Plan<768> { static constexpr int n = 3, r0 = 16, r1 = 16, r2 = 3; };
+template <> struct Plan<1536> { static constexpr int n = 3, r0 = 16, r1 = 16, r2 = 6; };
+
+template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, typename LD, typename ST>
+__device__ __forceinline__ void fft_fixed(int nl, const cxd* __restrict__ tw, cxd* sh, const LD& src, const ST& dst) {
+  using PL = Plan<N>;
+  const ShLines L = {sh, N + 1};
+  if constexpr (PL::n == 1) {
+    fft_stage_io<PL::r0, S, PPT, SRC_SH && DST_SH>(N, nl, 1, tw, src, dst);
+  } else if constexpr (PL::n == 2) {
+    fft_stage_io<PL::r0, S, PPT, SRC_SH>(N, nl, 1, tw, src, L);
+    __syncthreads();
+    fft_stage_io<PL::r1, S, PPT, DST_SH>(N, nl, PL::r0, tw, L, dst);
+  } else {
+    fft_stage_io<PL::r0, S, PPT, SRC_SH>(N, nl, 1, tw, src, L);
+    __syncthreads();
+    fft_stage_io<PL::r1, S, PPT, true>(N, nl, PL::r0, tw, L, L);
+    __syncthreads();
+    fft_stage_io<PL::r2, S, PPT, DST_SH>(N, nl, PL::r0 * PL::r1, tw, L, dst);
+  }
+}
+
+// NT > 0: the compile-time plan of length NT; NT = 0: the runtime plan of N.
+template <int NT, int S, int PPT, bool SRC_SH, bool DST_SH, typename LD, typename ST>
+__device__ __forceinline__ void fft_sel(int N, int nl, const cxd* __restrict__ tw, cxd* sh, const LD& src,
+                                        const ST& dst) {
+  if constexpr (NT > 0) {
+    fft_fixed<NT, S, PPT, SRC_SH, DST_SH>(nl, tw, sh, src, dst);
+  } else {
+    fft_global<S, PPT, SRC_SH, DST_SH>(N, nl, tw, sh, src, dst);
   }
 }
 

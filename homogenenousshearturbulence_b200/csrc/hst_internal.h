@@ -26,12 +26,14 @@ struct DeviceState {
   double2* Pp;          // x-forward of the products: [6][nzd][ny/Ty][nxB][Ty]
   double2* Q;           // spectral products: [6][ncol][ny]
   double* der;          // der(0:ny-1, 0:3, -2:2)
+  double* derS;         // the same, slab-major for the line-solve groups (SlabDer)
   double* y;            // y(-2:ny+1)
   double* dyl;          // dyl(0:ny-1)
   double* gdamp;        // gdamp(-nz:nz, 0:nx)
   double2* twx;         // exp(-2 pi i e / (2 nxd))
   double2* twz;         // exp(-2 pi i e / nzd)
   unsigned long long* cfl;  // running max (bits of a non-negative double)
+  int* err;                 // set by a kernel whose bounded wait ran out
 };
 
 // Scalars of one substep of the column kernel.
@@ -52,12 +54,18 @@ struct PhysScalars {
 cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st);
 cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int want_cfl, cudaStream_t st);
 cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st);
+// part: 0 the fused column kernel, 1 its right-hand-side stage alone (row
+// streaming, into RHS1/RHS2), 2 the rest (shift, solves, u, w) from RHS1/RHS2
 cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysScalars& ph, const SubstepScalars& sc,
-                          int exact, int nonlin, cudaStream_t st);
+                          int exact, int nonlin, int part, cudaStream_t st);
 cudaError_t launch_line_solve(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int sys, double lambda,
                               int src, int dst, double sx, double sz, cudaStream_t st);
 cudaError_t launch_fill_ghosts(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int field, double sx,
                                double sz, cudaStream_t st);
 size_t column_smem_bytes(const Geometry& g, int exact);
+// the constant twiddles of the register DFTs, once per device
+cudaError_t set_fft_constants();
+// a transform length the FFT kernels support
+bool fft_length_ok(int n);
 
 }  // namespace hst

@@ -1,0 +1,147 @@
+// The right-hand sides of one row of one Fourier column:
+// buildrhs_prepare (src/hst_equations.f90:92-141), buildrhs for both product
+// groups (:151-213), the hard damping mask (src/hst_damping.f90:119-133) and
+// the default mean-shear phase shift (src/hst_equations.f90:245-257).  The
+// taps of the five-point stencils come through accessors, so the same
+// arithmetic serves the kernels that read global memory and the one that
+// reads tiles staged in shared memory.
+#pragma once
+#include "hst_dev.cuh"
+#include "hst_internal.h"
+
+namespace hst {
+
+// what a column needs, uniform over its rows
+struct ColConst {
+  double al, be, kk, ni, S, gs, kappa;
+  bool c00, masked;
+  cxd ph_t;  // wrap phase at t: ghost images of the product rows
+};
+
+__device__ __forceinline__ ColConst col_const(int col, const Geometry& g, const PhysScalars& ps,
+                                              const SubstepScalars& sc, const double* __restrict__ gdamp) {
+  ColConst c;
+  const int ix = col / g.nzT, iz = col - ix * g.nzT - g.nz;
+  c.c00 = (ix == 0 && iz == 0);
+  c.al = ps.alfa0 * ix;
+  c.be = ps.beta0 * iz;
+  c.kk = c.al * c.al + c.be * c.be;
+  c.ni = ps.ni;
+  c.S = ps.S;
+  const double gcol = gdamp[col];
+  c.gs = sc.gsoft * gcol;
+  c.masked = sc.damp_hard && gcol > 0.0;
+  c.kappa = sc.s2now * c.al - ps.S * c.be;  // (s2 i alfa - S i beta) / i
+  c.ph_t = cexpi(-(c.al * sc.sx_t + c.be * sc.sz_t));
+  return c;
+}
+
+// TV(c, j): component c of V at row r + j - 2; TQ(p, j): product p at row
+// r + j - 2 (ghost phase applied); yr: y(r).  EXACT: no phase shift here
+// (shift_unweighted follows in the solve kernel).
+template <bool NONLIN, bool EXACT, class TV, class TQ>
+__device__ __forceinline__ void rhs_point(const ColConst& c, const SubstepScalars& sc, const double* __restrict__ der,
+                                          int ny, int r, double yr, const TV& tv, const TQ& tq, cxd o1in, cxd o2in,
+                                          cxd& r1, cxd& r2, cxd& o1, cxd& o2) {
+  const double kk = c.kk, al = c.al, be = c.be, ni = c.ni, gs = c.gs;
+  double d0[5], d1[5], d2[5], d4[5];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    d0[j] = derv(der, ny, r, 0, j - 2);
+    d1[j] = derv(der, ny, r, 1, j - 2);
+    d2[j] = derv(der, ny, r, 2, j - 2);
+    d4[j] = derv(der, ny, r, 3, j - 2);
+  }
+  // v equation
+  cxd unkn = mkc(0, 0), impl = mkc(0, 0);
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    double helm = d2[j] - kk * d0[j];
+    double biharm = d4[j] - 2.0 * kk * d2[j] + kk * kk * d0[j];
+    cxd v = tv(1, j);
+    unkn = mkc(unkn.x + helm * v.x, unkn.y + helm * v.y);
+    double nb = ni * biharm;
+    impl = mkc(impl.x + nb * v.x, impl.y + nb * v.y);
+  }
+  r2 = mkc((sc.ode0 * unkn.x) / sc.deltat + impl.x - sc.ode2 * o2in.x - (sc.ode1 * gs) * unkn.x,
+           (sc.ode0 * unkn.y) / sc.deltat + impl.y - sc.ode2 * o2in.y - (sc.ode1 * gs) * unkn.y);
+  o2 = mkc(-gs * unkn.x, -gs * unkn.y);
+  // eta equation (mean column: u, w packed)
+  unkn = mkc(0, 0);
+  impl = mkc(0, 0);
+  cxd expl = mkc(0, 0);
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    double helm = d2[j] - kk * d0[j];
+    cxd v1 = tv(0, j), v3 = tv(2, j), v2 = tv(1, j);
+    cxd f;
+    double w;
+    if (c.c00) {
+      f = mkc(v1.x, v3.x);
+      w = ni * d2[j];
+    } else {
+      f = mkc(-be * v1.y + al * v3.y, be * v1.x - al * v3.x);
+      w = ni * helm;
+    }
+    unkn = mkc(unkn.x + d0[j] * f.x, unkn.y + d0[j] * f.y);
+    impl = mkc(impl.x + w * f.x, impl.y + w * f.y);
+    double kd = c.kappa * d0[j];
+    expl = mkc(expl.x - kd * v2.y, expl.y + kd * v2.x);
+  }
+  expl = mkc(expl.x - gs * unkn.x, expl.y - gs * unkn.y);
+  r1 = mkc((sc.ode0 * unkn.x) / sc.deltat + impl.x - sc.ode2 * o1in.x + sc.ode1 * expl.x,
+           (sc.ode0 * unkn.y) / sc.deltat + impl.y - sc.ode2 * o1in.y + sc.ode1 * expl.y);
+  o1 = expl;
+  if (NONLIN) {
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+      cxd q0 = mkc(0, 0), q1 = mkc(0, 0), q2 = mkc(0, 0);
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        cxd qv = tq(p, j);
+        q0 = mkc(q0.x + d0[j] * qv.x, q0.y + d0[j] * qv.y);
+        q1 = mkc(q1.x + d1[j] * qv.x, q1.y + d1[j] * qv.y);
+        q2 = mkc(q2.x + d2[j] * qv.x, q2.y + d2[j] * qv.y);
+      }
+      cxd ru = mkc(0, 0), rw = mkc(0, 0), ex;
+      if (p == 0) {  // uu
+        ru = mkc(al * q0.y, -al * q0.x);
+        ex = cscale(-(al * al), q1);
+      } else if (p == 1) {  // vv
+        ex = cscale(kk, q1);
+      } else if (p == 2) {  // ww
+        rw = mkc(be * q0.y, -be * q0.x);
+        ex = cscale(-(be * be), q1);
+      } else if (p == 3) {  // uv
+        ru = cneg(q1);
+        ex = mkc(-al * q2.y + -(al * kk) * q0.y, al * q2.x + (al * kk) * q0.x);
+      } else if (p == 4) {  // vw
+        rw = cneg(q1);
+        ex = mkc(-be * q2.y + -(be * kk) * q0.y, be * q2.x + (be * kk) * q0.x);
+      } else {  // uw
+        ru = mkc(be * q0.y, -be * q0.x);
+        rw = mkc(al * q0.y, -al * q0.x);
+        ex = cscale(-((2.0 * al) * be), q1);
+      }
+      r2 = mkc(r2.x + sc.ode1 * ex.x, r2.y + sc.ode1 * ex.y);
+      o2 = cadd(o2, ex);
+      cxd e;
+      if (c.c00) e = mkc(ru.x, rw.x);
+      else e = mkc(-be * ru.y + al * rw.y, be * ru.x - al * rw.x);
+      r1 = mkc(r1.x + sc.ode1 * e.x, r1.y + sc.ode1 * e.y);
+      o1 = cadd(o1, e);
+    }
+  }
+  if (c.masked) {  // damping_mask
+    r1 = r2 = o1 = o2 = mkc(0, 0);
+  }
+  if (!EXACT) {  // shear_shift, default form
+    cxd f = cexpi(-(al * sc.dgx + be * sc.dgz) * yr);
+    r1 = cmul(r1, f);
+    r2 = cmul(r2, f);
+    o1 = cmul(o1, f);
+    o2 = cmul(o2, f);
+  }
+}
+
+}  // namespace hst

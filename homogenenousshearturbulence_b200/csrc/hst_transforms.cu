@@ -1,0 +1,272 @@
+// The transform kernels of the hst substep (FP64):
+//
+//   k_zinv   V (u, v, w) -> zero-padded z-inverse transform (Z)
+//   k_xprod  Z -> x-inverse (c2r) of u, v, w; the six products times
+//            1/(2 nxd nzd); the CFL maximum; x-forward (r2c) of the products
+//            truncated to the nx+1 retained modes (Pp)
+//   k_zfwd   Pp -> z-forward transform truncated to the 2nz+1 modes (Q)
+//
+// Together they are transform_to_physical + build_products (both groups) +
+// products_to_spectral + compute_cfl of the reference
+// (src/hst_transforms.f90:33-179, src/hst_fft.f90:181-237), with the local
+// transposes (src/hst_mpi.f90:615-669) absorbed into the index maps.  Only
+// the ny interior rows are transformed (see k_column for the ghost-row
+// products).  Z and Pp are stored [component][y tile][kz][ix][Ty]: a block
+// of k_zinv / k_zfwd (one x mode, one y tile, all kz) then spans a few
+// huge pages instead of one page per kz.
+#include "hst_dev.cuh"
+#include "hst_fft.cuh"
+#include "hst_internal.h"
+
+namespace hst {
+
+cudaError_t set_fft_constants() {
+  double2 w[48];
+  for (int k = 0; k < 48; ++k) {
+    long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / 48.0L;
+    w[k] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  return cudaMemcpyToSymbol(c_w48, w, sizeof w);
+}
+
+bool fft_length_ok(int n) { return plan_ok(n); }
+
+// --------------------------------------------------------------- k_zinv ----
+// assemble_vvdz + IFT (src/hst_transforms.f90:33-54, src/hst_fft.f90:195-207):
+// line yi of the block is row y0 + yi of one x mode of one component; the
+// z modes -nz..nz sit at padded index iz (iz >= 0) or nzd + iz.
+struct ZinvSrc {
+  const double2* __restrict__ col;  // V + (ix nzT) rows + 2 + y0: row y0 of iz = -nz
+  int rows, nz, NZ;
+  __device__ __forceinline__ cxd operator()(int yi, int kz) const {
+    int iz;
+    if (kz <= nz) iz = kz;
+    else if (kz >= NZ - nz) iz = kz - NZ;
+    else return mkc(0.0, 0.0);
+    return col[(size_t)(iz + nz) * rows + yi];
+  }
+};
+struct TileDst {  // one (component, y tile, x mode) z-line set of Z / Pp
+  double2* __restrict__ base;
+  size_t zstride;
+  __device__ __forceinline__ void operator()(int yi, int kz, cxd v) const { base[(size_t)kz * zstride + yi] = v; }
+};
+struct TileSrc {
+  const double2* __restrict__ base;
+  size_t zstride;
+  __device__ __forceinline__ cxd operator()(int yi, int kz) const { return base[(size_t)kz * zstride + yi]; }
+};
+
+template <int NT, int PPT>
+__global__ void __launch_bounds__(256) k_zinv(Geometry g, const double2* __restrict__ V0,
+                                              const double2* __restrict__ V1, const double2* __restrict__ V2,
+                                              double2* __restrict__ Z, const double2* __restrict__ twz) {
+  extern __shared__ double2 sh[];
+  const int yt = blockIdx.x, ix = blockIdx.y, c = blockIdx.z;
+  const int Ty = g.Ty, NZ = g.nzd, nyT = g.ny / Ty;
+  const double2* V = c == 0 ? V0 : (c == 1 ? V1 : V2);
+  const ZinvSrc src = {V + (size_t)ix * g.nzT * g.rows + 2 + yt * Ty, g.rows, g.nz, NZ};
+  const TileDst dst = {Z + (((size_t)c * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
+  fft_sel<NT, +1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
+}
+
+// --------------------------------------------------------------- k_zfwd ----
+// transpose_xTOz + FFT (src/hst_transforms.f90:135-139, src/hst_fft.f90:181-193)
+// keeping the 2nz+1 retained modes, stored without ghost rows.
+struct ZfwdDst {
+  double2* __restrict__ base;  // Q + (p ncol + ix nzT) ny + y0
+  int ny, nz, NZ;
+  __device__ __forceinline__ void operator()(int yi, int k, cxd v) const {
+    int iz;
+    if (k <= nz) iz = k;
+    else if (k >= NZ - nz) iz = k - NZ;
+    else return;
+    base[(size_t)(iz + nz) * ny + yi] = v;
+  }
+};
+
+template <int NT, int PPT>
+__global__ void __launch_bounds__(256) k_zfwd(Geometry g, const double2* __restrict__ Pp, double2* __restrict__ Q,
+                                              const double2* __restrict__ twz) {
+  extern __shared__ double2 sh[];
+  const int yt = blockIdx.x, ix = blockIdx.y, p = blockIdx.z;
+  const int Ty = g.Ty, NZ = g.nzd, nyT = g.ny / Ty;
+  const TileSrc src = {Pp + (((size_t)p * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
+  const ZfwdDst dst = {Q + ((size_t)p * g.ncol + (size_t)ix * g.nzT) * g.ny + yt * Ty, g.ny, g.nz, NZ};
+  fft_sel<NT, -1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
+}
+
+// -------------------------------------------------------------- k_xprod ----
+// to_x_points (zero padding + RFT), build_products for both groups,
+// compute_cfl and HFT of the products (src/hst_transforms.f90:85-133,
+// 163-179; src/hst_fft.f90:211-237) for one pair of rows at one z point.
+// Two real lines ride on one complex line: u + i v of each row and w0 + i w1
+// of the pair on the way in; (uu, vv), (ww, uv), (vw, uw) of each row on
+// the way out, separated by Hermitian symmetry.  The c2r reads only the
+// real part of the kx = 0 mode, as FFTW's and cuFFT's c2r do.
+struct XinvSrc {
+  const double2* __restrict__ zb;  // Z tile of component 0 at (y tile, kz), + row offset in the tile
+  size_t cs;                       // component stride of Z
+  int Ty, nx, NX;
+  __device__ __forceinline__ cxd operator()(int l, int k) const {
+    const int m = k <= nx ? k : (k >= NX - nx ? NX - k : -1);
+    if (m < 0) return mkc(0.0, 0.0);
+    const double2* p = zb + (size_t)m * Ty;
+    cxd a, b;
+    if (l == 0) {  // u(y0) + i v(y0)
+      a = p[0];
+      b = p[cs];
+    } else if (l == 1) {  // u(y1) + i v(y1)
+      a = p[1];
+      b = p[cs + 1];
+    } else {  // w(y0) + i w(y1)
+      a = p[2 * cs];
+      b = p[2 * cs + 1];
+    }
+    if (k == 0) return mkc(a.x, b.x);
+    if (k <= nx) return mkc(a.x - b.y, a.y + b.x);
+    return mkc(a.x + b.y, b.x - a.y);  // conj(a) + i conj(b)
+  }
+};
+// the products of row yy, pair pl (0: uu, vv; 1: ww, uv; 2: vw, uw) at x
+struct ProdSrc {
+  const cxd* sh;
+  int LS;
+  double f;
+  __device__ __forceinline__ cxd operator()(int l, int x) const {
+    const int yy = l >= 3 ? 1 : 0, pl = l - 3 * yy;
+    const cxd a = sh[yy * LS + x], b = sh[2 * LS + x];
+    const double u = a.x, v = a.y, w = yy ? b.y : b.x;
+    if (pl == 0) return mkc(u * u * f, v * v * f);
+    if (pl == 1) return mkc(w * w * f, u * v * f);
+    return mkc(v * w * f, u * w * f);
+  }
+};
+
+template <int NT, int PPT>
+__global__ void __launch_bounds__(320) k_xprod(Geometry g, const double2* __restrict__ Z, double2* __restrict__ Pp,
+                                               const double2* __restrict__ twx, const double* __restrict__ dyl,
+                                               PhysScalars ps, int want_cfl, unsigned long long* __restrict__ cflmax) {
+  extern __shared__ double2 sh[];
+  const int NX = 2 * g.nxd, nx = g.nx, nxB = g.nxB, NZ = g.nzd, Ty = g.Ty, LS = NX + 1;
+  const int nyT = g.ny / Ty;
+  const int y0 = 2 * blockIdx.x, kz = blockIdx.y;
+  const int yt = y0 / Ty, yi0 = y0 - yt * Ty;
+  const size_t cs = (size_t)NZ * nyT * nxB * Ty;
+  const size_t tile = ((size_t)yt * NZ + kz) * nxB * Ty;
+  const ShLines L = {sh, LS};
+  // u + i v of both rows and w0 + i w1 on the physical x grid
+  const XinvSrc xs = {Z + tile + yi0, cs, Ty, nx, NX};
+  fft_sel<NT, +1, PPT, false, true>(NX, 3, twx, sh, xs, L);
+  __syncthreads();
+  if (want_cfl) {
+    double cm = 0.0;
+    const double rdy0 = dyl[y0], rdy1 = dyl[y0 + 1];
+    for (int x = threadIdx.x; x < NX; x += blockDim.x) {
+      cxd a0 = sh[x], a1 = sh[LS + x], b = sh[2 * LS + x];
+      double c0 = fabs(a0.x) / ps.dx + fabs(a0.y) / rdy0 + fabs(b.x) / ps.dz;
+      double c1 = fabs(a1.x) / ps.dx + fabs(a1.y) / rdy1 + fabs(b.y) / ps.dz;
+      cm = fmax(cm, fmax(c0, c1));
+    }
+    for (int o = 16; o > 0; o >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(cflmax, (unsigned long long)__double_as_longlong(cm));
+  }
+  // the six product lines, transformed forward in place
+  const ProdSrc ps6 = {sh, LS, ps.factor};
+  fft_sel<NT, -1, PPT, true, true>(NX, 6, twx, sh, ps6, L);
+  __syncthreads();
+  // separate the two real transforms of each line, keep kx = 0..nx
+  for (int e = threadIdx.x; e < nxB * 3; e += blockDim.x) {
+    int pl = e / nxB, ix = e - pl * nxB;
+#pragma unroll
+    for (int yy = 0; yy < 2; ++yy) {
+      const cxd* Lp = sh + (pl + 3 * yy) * LS;
+      cxd Zk = Lp[ix], Zm = Lp[ix == 0 ? 0 : NX - ix];
+      cxd X = mkc(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y));
+      cxd Y = mkc(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x));
+      size_t o = tile + (size_t)ix * Ty + yi0 + yy;
+      Pp[(size_t)(2 * pl) * cs + o] = X;
+      Pp[(size_t)(2 * pl + 1) * cs + o] = Y;
+    }
+  }
+}
+
+// -------------------------------------------------------------- launchers ----
+static int fft_threads(int points, int ppt) {
+  int t = (points + ppt - 1) / ppt;
+  t = (t + 31) / 32 * 32;
+  return t < 64 ? 64 : t;
+}
+
+template <typename K>
+static void big_smem(K k) {
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+}
+
+// Dispatch on the transform length: compile-time plans for the lengths the
+// configurations use (16 points a thread up to 384, 32 above, so that a
+// block has at most 256 threads for up to 8 lines), the runtime plan
+// otherwise.
+#define HST_FFT_DISPATCH(N, PTS, CALL)                      \
+  do {                                                      \
+    switch (N) {                                            \
+      case 12: CALL(12, 16) break;                          \
+      case 24: CALL(24, 16) break;                          \
+      case 48: CALL(48, 16) break;                          \
+      case 96: CALL(96, 16) break;                          \
+      case 192: CALL(192, 16) break;                        \
+      case 384: CALL(384, 16) break;                        \
+      case 768: CALL(768, 32) break;                        \
+      case 1536: CALL(1536, 32) break;                      \
+      default:                                              \
+        if ((PTS) <= 16 * 256) CALL(0, 16) else CALL(0, 32) \
+        break;                                              \
+    }                                                       \
+  } while (0)
+
+cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st) {
+  const int pts = g.nzd * g.Ty;
+  const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(double2);
+  const dim3 grid(g.ny / g.Ty, g.nxB, 3);
+#define HST_ZINV(NT, PPT)                                                                               \
+  {                                                                                                     \
+    big_smem(k_zinv<NT, PPT>);                                                                          \
+    k_zinv<NT, PPT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], d.Z, d.twz); \
+  }
+  HST_FFT_DISPATCH(g.nzd, pts, HST_ZINV);
+#undef HST_ZINV
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st) {
+  const int pts = g.nzd * g.Ty;
+  const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(double2);
+  const dim3 grid(g.ny / g.Ty, g.nxB, 6);
+#define HST_ZFWD(NT, PPT)                                                            \
+  {                                                                                  \
+    big_smem(k_zfwd<NT, PPT>);                                                       \
+    k_zfwd<NT, PPT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Pp, d.Q, d.twz); \
+  }
+  HST_FFT_DISPATCH(g.nzd, pts, HST_ZFWD);
+#undef HST_ZFWD
+  return cudaGetLastError();
+}
+
+cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int want_cfl,
+                         cudaStream_t st) {
+  const int NX = 2 * g.nxd;
+  const int pts = 6 * NX;
+  const size_t smem = (size_t)6 * (NX + 1) * sizeof(double2);
+  const dim3 grid(g.ny / 2, g.nzd);
+#define HST_XPROD(NT, PPT)                                                                           \
+  {                                                                                                  \
+    big_smem(k_xprod<NT, PPT>);                                                                      \
+    k_xprod<NT, PPT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Z, d.Pp, d.twx, d.dyl, ph,      \
+                                                                 want_cfl, d.cfl);                   \
+  }
+  HST_FFT_DISPATCH(NX, pts, HST_XPROD);
+#undef HST_XPROD
+  return cudaGetLastError();
+}
+
+}  // namespace hst

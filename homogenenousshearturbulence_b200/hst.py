@@ -146,6 +146,27 @@ def read_deck(path) -> dict:
     return deck
 
 
+def fft_fit(n: int) -> bool:
+    """A power of two times at most one factor three (src/hst_input.f90:107-115)."""
+    j = n
+    while j % 2 == 0:
+        j //= 2
+    return j in (1, 3)
+
+
+def padded_sizes(nx, nz, nxd=0, nzd=0):
+    """nxd, nzd as read_input derives them (src/hst_input.f90:210-211)."""
+    if nxd <= 0:
+        nxd = 3 * (nx + 1) // 2
+        while not fft_fit(nxd):
+            nxd += 1
+    if nzd <= 0:
+        nzd = 3 * nz
+        while not fft_fit(nzd):
+            nzd += 1
+    return nxd, nzd
+
+
 # --------------------------------------------------------------- solver ----
 class Solver:
     """One field resident on one GPU (one hst_ctx)."""
@@ -175,7 +196,7 @@ class Solver:
         if rc != 0:
             raise HstError(f"hst_gpu_create failed ({rc}) for nx={p.nx} ny={p.ny} nz={p.nz}")
         self.nx, self.ny, self.nz = p.nx, p.ny, p.nz
-        self.nxd, self.nzd = p.nxd, p.nzd
+        self.nxd, self.nzd = padded_sizes(p.nx, p.nz, p.nxd, p.nzd)
         self.shape = (self.nx + 1, 2 * self.nz + 1, self.ny + 4)
         self.time = float(cfg.get("time", 0.0))
         self.deltat = float(cfg.get("deltat", 0.0))
@@ -300,7 +321,7 @@ class Solver:
     def s2_integral(self, t1, t2):
         return lib().hst_gpu_s2_integral(self._h, float(t1), float(t2))
 
-    KERNEL_CLASSES = ("zinv", "xprod", "zfwd", "column", "line_solve", "ghosts")
+    KERNEL_CLASSES = ("zinv", "xprod", "zfwd", "column", "line_solve", "ghosts", "rhs")
 
     def set_profiling(self, on: bool):
         self._check(lib().hst_gpu_set_profiling(self._h, int(bool(on))), "set_profiling")

@@ -43,6 +43,7 @@ extern "C" {
 #define HST_EARG (-1)    /* bad argument or unsupported size */
 #define HST_ENOMEM (-2)  /* device allocation refused */
 #define HST_ECUDA (-3)   /* CUDA runtime error */
+#define HST_ETIMEOUT (-4) /* a kernel's bounded wait ran out (the step's results are invalid) */
 #define HST_EFINITE (-5) /* non-finite CFL (the field blew up) */
 
 /* field ids: the three components of V, the carried explicit terms and the
@@ -143,7 +144,8 @@ double hst_gpu_s2_integral(const hst_ctx* ctx, double t1, double t2);
 #define HST_KC_COLUMN 3     /* the fused column kernel (right-hand sides, shift, solves, u, w) */
 #define HST_KC_LINE_SOLVE 4 /* hst_gpu_line_solve */
 #define HST_KC_GHOSTS 5     /* hst_gpu_fill_ghosts */
-#define HST_KC_N 6
+#define HST_KC_RHS 6        /* the right-hand sides streamed row by row (when the column stage is split) */
+#define HST_KC_N 7
 
 /* Per-kernel device time: with profiling on, every launch is bracketed by
  * two CUDA events on the context's stream; hst_gpu_kernel_times waits for
