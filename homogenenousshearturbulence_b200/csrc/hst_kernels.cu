@@ -355,7 +355,11 @@ __global__ void __launch_bounds__(32 * RT_WARPS) k_rhs_tiled(ColumnArgs a, int* 
   for (int t = 0; t < ntile; ++t) {
     const int stg = t & 1;
     if (!mbar_wait_bounded(&bar[stg], (t >> 1) & 1, RT_WAIT_LIMIT)) {
+      // record the failure, give this warp's copies still in flight a
+      // second bounded wait to land, and leave
       if (lane == 0) atomicExch(err, 1);
+      mbar_wait_bounded(&bar[stg], (t >> 1) & 1, RT_WAIT_LIMIT);
+      if (t + 1 < ntile) mbar_wait_bounded(&bar[stg ^ 1], ((t + 1) >> 1) & 1, RT_WAIT_LIMIT);
       return;
     }
     const double2* S = st0 + stg * RT_STAGE;
