@@ -5,7 +5,7 @@
 
 One step is one RK3 time step (three substeps, hst_gpu_timestep, with the
 CFL read-back the Fortran time loop does every step); the metric is
-substeps per second of the whole job.  Default workload: BASELINE config 2,
+substeps per second of the whole job.  Default workload:
 the plain FP64 drop-in at 384x384 dealiased x 256 (deck nx = 127, nz = 128,
 ny = 256; ly = 2 pi, alfa0 = beta0 = 1, S = 1, Re = 2000, dt = 0.002) from a
 seeded divergence-free field with E(k) ~ k^4 exp(-2 (k/8)^2), energy 0.1.
@@ -42,16 +42,16 @@ sys.path.insert(0, str(ROOT))
 
 PI = math.pi
 CONFIGS = {
-    # BASELINE config 1: 96^2 x 64, Re 1000, dt 0.005, k0 4
+    # 96^2 x 64, Re 1000, dt 0.005, k0 4
     "c1": dict(deck=dict(nx=31, ny=64, nz=32, alfa0=1.0, beta0=1.0, ly=2 * PI, re=1000.0, S=1.0, deltat=0.005),
-               k0=4.0, label="config 1: FP64 substep, 96x96 dealiased x 64 (nx=31, nz=32, ny=64), Re 1000, dt 0.005"),
-    # BASELINE config 2: 384^2 x 256, Re 2000, dt 0.002, k0 8
+               k0=4.0, label="FP64 substep, 96x96 dealiased x 64 (nx=31, nz=32, ny=64), Re 1000, dt 0.005"),
+    # 384^2 x 256, Re 2000, dt 0.002, k0 8
     "c2": dict(deck=dict(nx=127, ny=256, nz=128, alfa0=1.0, beta0=1.0, ly=2 * PI, re=2000.0, S=1.0, deltat=0.002),
-               k0=8.0, label="config 2: FP64 substep, 384x384 dealiased x 256 (nx=127, nz=128, ny=256), Re 2000, dt 0.002"),
-    # BASELINE config 3 geometry in FP64: 768^2 x 512, Re 5000, dt 0.001, exact_shift, k0 16
+               k0=8.0, label="FP64 substep, 384x384 dealiased x 256 (nx=127, nz=128, ny=256), Re 2000, dt 0.002"),
+    # 768^2 x 512 in FP64, Re 5000, dt 0.001, exact_shift, k0 16
     "c3": dict(deck=dict(nx=255, ny=512, nz=256, alfa0=1.0, beta0=1.0, ly=2 * PI, re=5000.0, S=1.0, deltat=0.001,
                          exact_shift=True),
-               k0=16.0, label="config 3 geometry, FP64: 768x768 dealiased x 512 (nx=255, nz=256, ny=512), exact_shift"),
+               k0=16.0, label="FP64 substep, 768x768 dealiased x 512 (nx=255, nz=256, ny=512), exact_shift"),
 }
 
 

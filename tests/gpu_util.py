@@ -67,7 +67,7 @@ def run_pair(s, o, dt, nsteps):
 
 
 def c1_deck(**over):
-    """96^2 x 64, ly = 2 pi, alfa0 = beta0 = 1, Re = 1000, dt = 0.005."""
+    """The 96^2 x 64 workload (deck nx = 31, nz = 32, ny = 64): ly = 2 pi, alfa0 = beta0 = 1, Re = 1000, dt = 0.005."""
     d = dict(nx=31, ny=64, nz=32, alfa0=1.0, beta0=1.0, ly=2.0 * PI, re=1000.0, S=1.0, deltat=0.005, cflmax=0.0)
     d.update(over)
     return d

@@ -37,8 +37,8 @@ def test_bad_sizes_are_rejected_without_a_device():
     assert hst.lib().hst_gpu_device_bytes(ct.byref(p)) == 0.0
 
 
-def test_device_bytes_of_the_benchmark_configs():
-    # 512^3 (config 3) must fit in one B200's 180 GB with room to spare
+def test_device_bytes_of_the_benchmark_workloads():
+    # the 768^2 x 512 workload must fit in one B200's 180 GB with room to spare
     b3 = hst.device_bytes(nx=255, ny=512, nz=256, alfa0=1.0, beta0=1.0, ly=6.283185307179586)
     assert 20e9 < b3 < 60e9
     b1 = hst.device_bytes(nx=31, ny=64, nz=32, alfa0=1.0, beta0=1.0, ly=6.283185307179586)

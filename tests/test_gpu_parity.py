@@ -132,10 +132,10 @@ def test_golden_regression(golden, name):
 # --------------------------------------------------- the FP64 substep path ----
 @pytest.mark.parametrize("variant", ["default", "exact_shift", "s2_exact", "damped_soft", "damped_hard", "stretched"])
 def test_c1_parity(variant):
-    """BASELINE config 1 (96x96x64 dealiased, ly = 2 pi, Re = 1000, dt =
+    """The 96x96x64 dealiased workload (ly = 2 pi, Re = 1000, dt =
     0.005, E(k) ~ k^4 exp(-2(k/4)^2), energy 0.1): 30 substeps on the GPU
     against the oracle, relative L2 over the interior rows <= 1e-12 (the
-    FP64 target), plus the branches config 1 does not take."""
+    FP64 target), plus the branches that workload does not take."""
     over = {}
     if variant == "exact_shift":
         over = dict(exact_shift=True)
