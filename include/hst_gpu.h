@@ -163,6 +163,25 @@ long long hst_gpu_launch_count(const hst_ctx* ctx);
 /* The stream the context queues its work on (a cudaStream_t). */
 void* hst_gpu_stream(const hst_ctx* ctx);
 
+/* ----------------------------------------------- no context, no allocation */
+/* line_solve(sys, lambda, src, dst, shift_x, shift_z) of hst_gpu_line_solve on
+ * fields in the caller's own device memory: src and dst are device pointers
+ * to one field each (the layout above, ghost rows included; src's ghosts
+ * filled when sys is HST_KIND_DY), der a device pointer to der(0:ny-1, 0:3,
+ * -2:2) in Fortran order; re gives ni = 1/re.  Queued on `stream` (a
+ * cudaStream_t, NULL for the default stream) on the current device.  No
+ * device memory is allocated: the working table lives in a static array of
+ * the library, one per device, which limits ny to 2048 (larger ny returns
+ * HST_EARG).  Calls on one device must not overlap in time (one stream, or
+ * ordered by events).  The first call on a device does set-up (it looks up
+ * the static array's address): make it before any stream capture begins.
+ * Errors: a negative HST_E* class, with a message in msg[0:msg_len) when msg
+ * is not NULL.  No counterpart in the reference, whose line_solve always
+ * works on its module arrays (src/hst_linsolve.f90:147). */
+int hst_gpu_line_solve_noalloc(int nx, int ny, int nz, double alfa0, double beta0, double re, int sys,
+                               double lambda, const double* der, const double* src, double* dst, double shift_x,
+                               double shift_z, void* stream, char* msg, int msg_len);
+
 #ifdef __cplusplus
 }
 #endif
