@@ -303,15 +303,26 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
   g.P = P;
   g.m = p.ny / P;
   g.MS = g.m | 1;
-  // transform y tile
+  // FFT points per thread: 8 selects the low-register plans (lengths 192,
+  // 384, 768; the x kernel then moves its tiles by TMA).  Measured at
+  // 384^2 x 256: x 8 (1.31 against 2.41 ms), z 16 (0.26/0.50 against
+  // 0.29/0.52 ms); at 768^2 x 512 the z kernels need 8 (2.4/4.9 against
+  // 4.0/14.0 ms).  HST_FFT_PPT_X / HST_FFT_PPT_Z override.
+  auto ppt_of = [](const char* name, int dflt) {
+    const char* e = std::getenv(name);
+    int v = e ? std::atoi(e) : dflt;
+    return (v == 8 || v == 16) ? v : dflt;
+  };
+  g.pptx = ppt_of("HST_FFT_PPT_X", 8);
+  g.pptz = ppt_of("HST_FFT_PPT_Z", g.nzd >= 768 ? 8 : 16);
+  // transform y tile (at most 512 threads for the 8-point z plans)
   g.Ty = 2;
   for (int t : {8, 4}) {
-    if (p.ny % t == 0 && (size_t)t * (g.nzd + 1) * 16 <= 100 * 1024) {
+    if (p.ny % t == 0 && (size_t)t * (g.nzd + 1) * 16 <= 100 * 1024 && (g.pptz != 8 || t * g.nzd / 8 <= 512)) {
       g.Ty = t;
       break;
     }
   }
-  g.ppt = 16;
   if (!hst::fft_length_ok(2 * g.nxd) || !hst::fft_length_ok(g.nzd) || g.Ty * g.nzd > 32 * 256 ||
       6 * 2 * g.nxd > 32 * 320) {
     why = "transform length not supported (2 nxd <= 1536, radices 2, 3, 4, 6, 8, 12, 16, 24)";
@@ -474,6 +485,7 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   cudaMemcpy(d.twx, tx.data(), sizeof(double2) * tx.size(), cudaMemcpyHostToDevice);
   cudaMemcpy(d.twz, tz.data(), sizeof(double2) * tz.size(), cudaMemcpyHostToDevice);
   cudaError_t e = hst::set_fft_constants();
+  if (e == cudaSuccess) e = hst::make_transform_maps(g, d);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -17,6 +17,8 @@
 // in extended precision.  Unnormalised both ways, like the reference's FFTW
 // and cuFFT plans (src/hst_fft.f90:98-121): S = -1 forward, S = +1 backward.
 #pragma once
+#include <type_traits>
+
 #include "hst_dev.cuh"
 
 namespace hst {
@@ -150,12 +152,22 @@ struct ShLines {
   __device__ __forceinline__ cxd operator()(int l, int i) const { return p[l * LS + i]; }
   __device__ __forceinline__ void operator()(int l, int i, cxd v) const { p[l * LS + i] = v; }
 };
+// The same with one pad element after every 8: with butterflies mapped
+// index-fastest (JF) the radix-8/6/12 exchanges of the 8-point plans are
+// then free of bank conflicts.  Line stride ls_padded(N).
+struct ShLinesP {
+  cxd* p;
+  int LS;
+  __device__ __forceinline__ cxd operator()(int l, int i) const { return p[l * LS + i + (i >> 3)]; }
+  __device__ __forceinline__ void operator()(int l, int i, cxd v) const { p[l * LS + i + (i >> 3)] = v; }
+};
+__host__ __device__ constexpr int ls_padded(int N) { return N + N / 8 + 1; }
 
 // One radix-R stage.  Butterfly b of the block: line l = b % nl, index
 // j = b / nl.  Inputs ld(l, j + r N/R), outputs st(l, (j/Ns) Ns R + j%Ns + r Ns).
 // SYNC: the stage reads and writes the same shared lines (all reads, then
 // a barrier, then all writes).
-template <int R, int S, int PPT, bool SYNC, typename LD, typename ST>
+template <int R, int S, int PPT, bool SYNC, typename LD, typename ST, bool JF = false>
 __device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const cxd* __restrict__ tw, const LD& ld,
                                              const ST& st) {
   constexpr int MAXB = (PPT + R - 1) / R;
@@ -169,7 +181,7 @@ __device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const cxd* _
     int b = threadIdx.x + k * blockDim.x;
     lj[k] = -1;
     if (b < total) {
-      int l = b % nl, j = b / nl;
+      int l = JF ? b / nb : b % nl, j = JF ? b % nb : b / nl;
       int kk = j % Ns;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
@@ -189,7 +201,7 @@ __device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const cxd* _
 #pragma unroll
   for (int k = 0; k < MAXB; ++k) {
     if (lj[k] >= 0) {
-      int l = lj[k] % nl, j = lj[k] / nl;
+      int l = JF ? lj[k] / nb : lj[k] % nl, j = JF ? lj[k] % nb : lj[k] / nl;
       int kk = j % Ns;
       int base = (j / Ns) * Ns * R + kk;
 #pragma unroll
@@ -255,31 +267,47 @@ template <> struct Plan<384> { static constexpr int n = 2, r0 = 16, r1 = 24, r2 
 template <> struct Plan<768> { static constexpr int n = 3, r0 = 16, r1 = 16, r2 = 3; };
 template <> struct Plan<1536> { static constexpr int n = 3, r0 = 16, r1 = 16, r2 = 6; };
 
-template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, typename LD, typename ST>
+// Plans of at most radix 12 for 8 points a thread: more stages (one more
+// shared exchange) for far fewer registers, hence more resident warps.
+template <int N>
+struct Plan8 {
+  static constexpr int n = 0, r0 = 1, r1 = 1, r2 = 1;
+};
+template <> struct Plan8<12> { static constexpr int n = 1, r0 = 12, r1 = 1, r2 = 1; };
+template <> struct Plan8<24> { static constexpr int n = 2, r0 = 4, r1 = 6, r2 = 1; };
+template <> struct Plan8<48> { static constexpr int n = 2, r0 = 8, r1 = 6, r2 = 1; };
+template <> struct Plan8<96> { static constexpr int n = 2, r0 = 8, r1 = 12, r2 = 1; };
+template <> struct Plan8<192> { static constexpr int n = 3, r0 = 8, r1 = 4, r2 = 6; };
+template <> struct Plan8<384> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 = 6; };
+template <> struct Plan8<768> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 = 12; };
+
+template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF, typename LD, typename ST>
 __device__ __forceinline__ void fft_fixed(int nl, const cxd* __restrict__ tw, cxd* sh, const LD& src, const ST& dst) {
-  using PL = Plan<N>;
-  const ShLines L = {sh, N + 1};
+  using PL = std::conditional_t<(PPT <= 8), Plan8<N>, Plan<N>>;
+  static_assert(PL::n > 0, "no compile-time plan for this length and points per thread");
+  using LT = std::conditional_t<JF, ShLinesP, ShLines>;
+  const LT L = {sh, JF ? ls_padded(N) : N + 1};
   if constexpr (PL::n == 1) {
-    fft_stage_io<PL::r0, S, PPT, SRC_SH && DST_SH>(N, nl, 1, tw, src, dst);
+    fft_stage_io<PL::r0, S, PPT, SRC_SH && DST_SH, LD, ST, JF>(N, nl, 1, tw, src, dst);
   } else if constexpr (PL::n == 2) {
-    fft_stage_io<PL::r0, S, PPT, SRC_SH>(N, nl, 1, tw, src, L);
+    fft_stage_io<PL::r0, S, PPT, SRC_SH, LD, LT, JF>(N, nl, 1, tw, src, L);
     __syncthreads();
-    fft_stage_io<PL::r1, S, PPT, DST_SH>(N, nl, PL::r0, tw, L, dst);
+    fft_stage_io<PL::r1, S, PPT, DST_SH, LT, ST, JF>(N, nl, PL::r0, tw, L, dst);
   } else {
-    fft_stage_io<PL::r0, S, PPT, SRC_SH>(N, nl, 1, tw, src, L);
+    fft_stage_io<PL::r0, S, PPT, SRC_SH, LD, LT, JF>(N, nl, 1, tw, src, L);
     __syncthreads();
-    fft_stage_io<PL::r1, S, PPT, true>(N, nl, PL::r0, tw, L, L);
+    fft_stage_io<PL::r1, S, PPT, true, LT, LT, JF>(N, nl, PL::r0, tw, L, L);
     __syncthreads();
-    fft_stage_io<PL::r2, S, PPT, DST_SH>(N, nl, PL::r0 * PL::r1, tw, L, dst);
+    fft_stage_io<PL::r2, S, PPT, DST_SH, LT, ST, JF>(N, nl, PL::r0 * PL::r1, tw, L, dst);
   }
 }
 
 // NT > 0: the compile-time plan of length NT; NT = 0: the runtime plan of N.
-template <int NT, int S, int PPT, bool SRC_SH, bool DST_SH, typename LD, typename ST>
+template <int NT, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF = false, typename LD, typename ST>
 __device__ __forceinline__ void fft_sel(int N, int nl, const cxd* __restrict__ tw, cxd* sh, const LD& src,
                                         const ST& dst) {
   if constexpr (NT > 0) {
-    fft_fixed<NT, S, PPT, SRC_SH, DST_SH>(nl, tw, sh, src, dst);
+    fft_fixed<NT, S, PPT, SRC_SH, DST_SH, JF>(nl, tw, sh, src, dst);
   } else {
     fft_global<S, PPT, SRC_SH, DST_SH>(N, nl, tw, sh, src, dst);
   }

@@ -1,6 +1,7 @@
 // Internal interface between the C ABI (hst_capi.cu) and the kernels
 // (hst_kernels.cu).  Not installed; the public interface is include/hst_gpu.h.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -17,7 +18,7 @@ struct Geometry {
   long nf;             // complex elements of one field (ncol * rows)
   int P, m, MS;        // line-solve group: P lanes, m rows per lane, slab stride
   int Ty;              // y tile of the transforms (divides ny)
-  int ppt;             // FFT points per thread
+  int pptx, pptz;      // FFT points per thread of the x and z transforms (8: the low-register plans)
 };
 
 struct DeviceState {
@@ -34,6 +35,10 @@ struct DeviceState {
   double2* twz;         // exp(-2 pi i e / nzd)
   unsigned long long* cfl;  // running max (bits of a non-negative double)
   int* err;                 // set by a kernel whose bounded wait ran out
+  // TMA maps of Z and Pp as 4-D f64 tensors {2 Ty, nxB, nzd ny/Ty, comps}
+  // (set by make_transform_maps when the x kernel's 8-point plan uses them)
+  CUtensorMap tmZ, tmPp;
+  bool maps;
 };
 
 // Scalars of one substep of the column kernel.
@@ -63,6 +68,8 @@ cudaError_t launch_line_solve(const Geometry& g, const DeviceState& d, const Phy
 cudaError_t launch_fill_ghosts(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int field, double sx,
                                double sz, cudaStream_t st);
 size_t column_smem_bytes(const Geometry& g, int exact);
+// the TMA maps of Z and Pp for the x kernel (d.maps false when not used)
+cudaError_t make_transform_maps(const Geometry& g, DeviceState& d);
 // the constant twiddles of the register DFTs, once per device
 cudaError_t set_fft_constants();
 // a transform length the FFT kernels support

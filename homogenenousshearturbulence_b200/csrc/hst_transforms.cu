@@ -58,7 +58,7 @@ struct TileSrc {
 };
 
 template <int NT, int PPT>
-__global__ void __launch_bounds__(256) k_zinv(Geometry g, const double2* __restrict__ V0,
+__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256) k_zinv(Geometry g, const double2* __restrict__ V0,
                                               const double2* __restrict__ V1, const double2* __restrict__ V2,
                                               double2* __restrict__ Z, const double2* __restrict__ twz) {
   extern __shared__ double2 sh[];
@@ -86,7 +86,7 @@ struct ZfwdDst {
 };
 
 template <int NT, int PPT>
-__global__ void __launch_bounds__(256) k_zfwd(Geometry g, const double2* __restrict__ Pp, double2* __restrict__ Q,
+__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256) k_zfwd(Geometry g, const double2* __restrict__ Pp, double2* __restrict__ Q,
                                               const double2* __restrict__ twz) {
   extern __shared__ double2 sh[];
   const int yt = blockIdx.x, ix = blockIdx.y, p = blockIdx.z;
@@ -128,14 +128,38 @@ struct XinvSrc {
     return mkc(a.x + b.y, b.x - a.y);  // conj(a) + i conj(b)
   }
 };
+// The same from the block's staging copy of the tile, [comp 3][nxB][row 2]
+// (landed by TMA)
+struct XinvSh {
+  const double2* s;
+  int nxB, nx, NX;
+  __device__ __forceinline__ cxd operator()(int l, int k) const {
+    const int m = k <= nx ? k : (k >= NX - nx ? NX - k : -1);
+    if (m < 0) return mkc(0.0, 0.0);
+    cxd a, b;
+    if (l == 0) {
+      a = s[2 * m];
+      b = s[2 * (nxB + m)];
+    } else if (l == 1) {
+      a = s[2 * m + 1];
+      b = s[2 * (nxB + m) + 1];
+    } else {
+      a = s[2 * (2 * nxB + m)];
+      b = s[2 * (2 * nxB + m) + 1];
+    }
+    if (k == 0) return mkc(a.x, b.x);
+    if (k <= nx) return mkc(a.x - b.y, a.y + b.x);
+    return mkc(a.x + b.y, b.x - a.y);
+  }
+};
 // the products of row yy, pair pl (0: uu, vv; 1: ww, uv; 2: vw, uw) at x
+template <typename LT>
 struct ProdSrc {
-  const cxd* sh;
-  int LS;
+  LT L;
   double f;
   __device__ __forceinline__ cxd operator()(int l, int x) const {
     const int yy = l >= 3 ? 1 : 0, pl = l - 3 * yy;
-    const cxd a = sh[yy * LS + x], b = sh[2 * LS + x];
+    const cxd a = L(yy, x), b = L(2, x);
     const double u = a.x, v = a.y, w = yy ? b.y : b.x;
     if (pl == 0) return mkc(u * u * f, v * v * f);
     if (pl == 1) return mkc(w * w * f, u * v * f);
@@ -143,27 +167,81 @@ struct ProdSrc {
   }
 };
 
+#ifndef XPROD_MINB
+#define XPROD_MINB 3
+#endif
+// launch bounds of k_xprod: 6 NX / PPT threads; the 8-point plan at 384
+// is held to 72 registers so that three 288-thread blocks fit an SM
+constexpr int xprod_threads(int NT, int PPT) { return PPT <= 8 ? (NT == 384 ? 288 : 640) : 320; }
+constexpr int xprod_min_blocks(int NT, int PPT) { return PPT <= 8 && NT == 384 ? XPROD_MINB : 1; }
+
+constexpr int XPROD_WAIT_LIMIT = 1 << 22;  // polls of the tile's TMA barrier before giving up
+
+// shared layout of the TMA variant (double2 units): the six padded lines,
+// then the staging tile (in: [3][nxB][2], out: [6][nxB][2]) rounded up to
+// the next 128-byte address (tensor copies need 128-byte aligned shared
+// addresses, and the dynamic shared base is only known to be 16-byte
+// aligned), then the mbarrier and the tile flag
+__host__ __device__ inline int xprod_stage_off(int NX) { return 6 * ls_padded(NX); }
+__host__ __device__ inline size_t xprod_tma_smem(int NX, int nxB) {
+  return ((size_t)xprod_stage_off(NX) + 12 * (size_t)nxB + 2) * sizeof(double2) + 128;
+}
+
 template <int NT, int PPT>
-__global__ void __launch_bounds__(320) k_xprod(Geometry g, const double2* __restrict__ Z, double2* __restrict__ Pp,
-                                               const double2* __restrict__ twx, const double* __restrict__ dyl,
-                                               PhysScalars ps, int want_cfl, unsigned long long* __restrict__ cflmax) {
+__global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, PPT))
+    k_xprod(Geometry g, const double2* __restrict__ Z, double2* __restrict__ Pp, const double2* __restrict__ twx,
+            const double* __restrict__ dyl, PhysScalars ps, int want_cfl, unsigned long long* __restrict__ cflmax,
+            const __grid_constant__ CUtensorMap tmZ, const __grid_constant__ CUtensorMap tmP, int* __restrict__ err) {
   extern __shared__ double2 sh[];
-  const int NX = 2 * g.nxd, nx = g.nx, nxB = g.nxB, NZ = g.nzd, Ty = g.Ty, LS = NX + 1;
+  // 8-point plans: butterflies index-fastest over padded shared lines, the
+  // tile in and out by TMA
+  constexpr bool JF = (PPT <= 8 && NT > 0);
+  using LT = std::conditional_t<JF, ShLinesP, ShLines>;
+  const int NX = 2 * g.nxd, nx = g.nx, nxB = g.nxB, NZ = g.nzd, Ty = g.Ty, LS = JF ? ls_padded(NX) : NX + 1;
   const int nyT = g.ny / Ty;
   const int y0 = 2 * blockIdx.x, kz = blockIdx.y;
   const int yt = y0 / Ty, yi0 = y0 - yt * Ty;
   const size_t cs = (size_t)NZ * nyT * nxB * Ty;
   const size_t tile = ((size_t)yt * NZ + kz) * nxB * Ty;
-  const ShLines L = {sh, LS};
+  const LT L = {sh, LS};
+  double2* stg = sh + xprod_stage_off(NX);
+  if constexpr (JF) stg += ((128u - (smem_u32(stg) & 127u)) & 127u) / sizeof(double2);
   // u + i v of both rows and w0 + i w1 on the physical x grid
-  const XinvSrc xs = {Z + tile + yi0, cs, Ty, nx, NX};
-  fft_sel<NT, +1, PPT, false, true>(NX, 3, twx, sh, xs, L);
+  if constexpr (JF) {
+    uint64_t* bar = reinterpret_cast<uint64_t*>(stg + 12 * nxB);
+    int& tile_ok = *reinterpret_cast<int*>(stg + 12 * nxB + 1);
+    if ((smem_u32(stg) & 127u) != 0) {  // never taken: the staging tile is aligned above
+      if (threadIdx.x == 0) atomicExch(err, 1);
+      return;
+    }
+    if (threadIdx.x == 0) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+      mbar_arrive_expect_tx(bar, 3u * nxB * 32u);
+      tma_load_4d(stg, &tmZ, 2 * yi0, 0, yt * NZ + kz, 0, bar);
+      bool ok = mbar_wait_bounded(bar, 0, XPROD_WAIT_LIMIT);
+      if (!ok) {
+        // record the failure and give the copy a second bounded wait
+        // before the block (and its shared memory) goes away
+        atomicExch(err, 1);
+        mbar_wait_bounded(bar, 0, XPROD_WAIT_LIMIT);
+      }
+      tile_ok = ok;
+    }
+    __syncthreads();
+    if (!tile_ok) return;
+    const XinvSh xs = {stg, nxB, nx, NX};
+    fft_sel<NT, +1, PPT, false, true, JF>(NX, 3, twx, sh, xs, L);
+  } else {
+    const XinvSrc xs = {Z + tile + yi0, cs, Ty, nx, NX};
+    fft_sel<NT, +1, PPT, false, true, JF>(NX, 3, twx, sh, xs, L);
+  }
   __syncthreads();
   if (want_cfl) {
     double cm = 0.0;
     const double rdy0 = dyl[y0], rdy1 = dyl[y0 + 1];
     for (int x = threadIdx.x; x < NX; x += blockDim.x) {
-      cxd a0 = sh[x], a1 = sh[LS + x], b = sh[2 * LS + x];
+      cxd a0 = L(0, x), a1 = L(1, x), b = L(2, x);
       double c0 = fabs(a0.x) / ps.dx + fabs(a0.y) / rdy0 + fabs(b.x) / ps.dz;
       double c1 = fabs(a1.x) / ps.dx + fabs(a1.y) / rdy1 + fabs(b.y) / ps.dz;
       cm = fmax(cm, fmax(c0, c1));
@@ -172,23 +250,76 @@ __global__ void __launch_bounds__(320) k_xprod(Geometry g, const double2* __rest
     if ((threadIdx.x & 31) == 0) atomicMax(cflmax, (unsigned long long)__double_as_longlong(cm));
   }
   // the six product lines, transformed forward in place
-  const ProdSrc ps6 = {sh, LS, ps.factor};
-  fft_sel<NT, -1, PPT, true, true>(NX, 6, twx, sh, ps6, L);
+  const ProdSrc<LT> ps6 = {L, ps.factor};
+  fft_sel<NT, -1, PPT, true, true, JF>(NX, 6, twx, sh, ps6, L);
   __syncthreads();
   // separate the two real transforms of each line, keep kx = 0..nx
   for (int e = threadIdx.x; e < nxB * 3; e += blockDim.x) {
     int pl = e / nxB, ix = e - pl * nxB;
 #pragma unroll
     for (int yy = 0; yy < 2; ++yy) {
-      const cxd* Lp = sh + (pl + 3 * yy) * LS;
-      cxd Zk = Lp[ix], Zm = Lp[ix == 0 ? 0 : NX - ix];
+      const int ln = pl + 3 * yy;
+      cxd Zk = L(ln, ix), Zm = L(ln, ix == 0 ? 0 : NX - ix);
       cxd X = mkc(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y));
       cxd Y = mkc(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x));
-      size_t o = tile + (size_t)ix * Ty + yi0 + yy;
-      Pp[(size_t)(2 * pl) * cs + o] = X;
-      Pp[(size_t)(2 * pl + 1) * cs + o] = Y;
+      if constexpr (JF) {
+        stg[((2 * pl) * nxB + ix) * 2 + yy] = X;
+        stg[((2 * pl + 1) * nxB + ix) * 2 + yy] = Y;
+      } else {
+        size_t o = tile + (size_t)ix * Ty + yi0 + yy;
+        Pp[(size_t)(2 * pl) * cs + o] = X;
+        Pp[(size_t)(2 * pl + 1) * cs + o] = Y;
+      }
     }
   }
+  if constexpr (JF) {
+    // the six spectra of both rows in one tensor store
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tma_store_4d(&tmP, 2 * yi0, 0, yt * NZ + kz, 0, stg);
+      bulk_commit();
+      bulk_wait_read_all();
+    }
+  }
+}
+
+// ------------------------------------------------------------- TMA maps ----
+// Z and Pp seen as 4-D f64 tensors: d0 = the 2 Ty doubles of one y tile
+// (innermost), d1 = ix, d2 = (y tile, kz) as yt nzd + kz, d3 = component.
+// The x kernel's box is {4 doubles (two rows), nxB, 1, comps}.
+static bool xprod_uses_maps(const Geometry& g) {
+  const int NX = 2 * g.nxd;
+  return g.pptx == 8 && (NX == 192 || NX == 384 || NX == 768) && g.nxB <= 256;
+}
+
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+cudaError_t make_transform_maps(const Geometry& g, DeviceState& d) {
+  d.maps = false;
+  if (!xprod_uses_maps(g)) return cudaSuccess;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return e != cudaSuccess ? e : cudaErrorNotSupported;
+  const EncodeTiled enc = reinterpret_cast<EncodeTiled>(fn);
+  const int nyT = g.ny / g.Ty;
+  for (int which = 0; which < 2; ++which) {
+    const cuuint32_t comps = which == 0 ? 3 : 6;
+    cuuint64_t dims[4] = {(cuuint64_t)2 * g.Ty, (cuuint64_t)g.nxB, (cuuint64_t)g.nzd * nyT, comps};
+    cuuint64_t strides[3] = {(cuuint64_t)16 * g.Ty, (cuuint64_t)16 * g.Ty * g.nxB,
+                             (cuuint64_t)16 * g.Ty * g.nxB * g.nzd * nyT};
+    cuuint32_t box[4] = {4, (cuuint32_t)g.nxB, 1, comps};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(which == 0 ? &d.tmZ : &d.tmPp, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+                     which == 0 ? (void*)d.Z : (void*)d.Pp, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  }
+  d.maps = true;
+  return cudaSuccess;
 }
 
 // -------------------------------------------------------------- launchers ----
@@ -204,19 +335,21 @@ static void big_smem(K k) {
 }
 
 // Dispatch on the transform length: compile-time plans for the lengths the
-// configurations use (16 points a thread up to 384, 32 above, so that a
-// block has at most 256 threads for up to 8 lines), the runtime plan
-// otherwise.
-#define HST_FFT_DISPATCH(N, PTS, CALL)                      \
+// workloads use, with 8 points a thread (radix <= 12, P8) or 16 up to 384
+// and 32 above (radix 16/24), the runtime plan otherwise.
+#define HST_FFT_DISPATCH(N, PTS, P8, CALL)                  \
   do {                                                      \
     switch (N) {                                            \
       case 12: CALL(12, 16) break;                          \
       case 24: CALL(24, 16) break;                          \
       case 48: CALL(48, 16) break;                          \
       case 96: CALL(96, 16) break;                          \
-      case 192: CALL(192, 16) break;                        \
-      case 384: CALL(384, 16) break;                        \
-      case 768: CALL(768, 32) break;                        \
+      case 192:                                             \
+        if (P8) CALL(192, 8) else CALL(192, 16) break;      \
+      case 384:                                             \
+        if (P8) CALL(384, 8) else CALL(384, 16) break;      \
+      case 768:                                             \
+        if (P8) CALL(768, 8) else CALL(768, 32) break;      \
       case 1536: CALL(1536, 32) break;                      \
       default:                                              \
         if ((PTS) <= 16 * 256) CALL(0, 16) else CALL(0, 32) \
@@ -233,7 +366,7 @@ cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st
     big_smem(k_zinv<NT, PPT>);                                                                          \
     k_zinv<NT, PPT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], d.Z, d.twz); \
   }
-  HST_FFT_DISPATCH(g.nzd, pts, HST_ZINV);
+  HST_FFT_DISPATCH(g.nzd, pts, g.pptz == 8, HST_ZINV);
 #undef HST_ZINV
   return cudaGetLastError();
 }
@@ -247,7 +380,7 @@ cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st
     big_smem(k_zfwd<NT, PPT>);                                                       \
     k_zfwd<NT, PPT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Pp, d.Q, d.twz); \
   }
-  HST_FFT_DISPATCH(g.nzd, pts, HST_ZFWD);
+  HST_FFT_DISPATCH(g.nzd, pts, g.pptz == 8, HST_ZFWD);
 #undef HST_ZFWD
   return cudaGetLastError();
 }
@@ -256,15 +389,16 @@ cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScal
                          cudaStream_t st) {
   const int NX = 2 * g.nxd;
   const int pts = 6 * NX;
-  const size_t smem = (size_t)6 * (NX + 1) * sizeof(double2);
+  const size_t smem = xprod_uses_maps(g) ? xprod_tma_smem(NX, g.nxB) : (size_t)6 * (NX + 1) * sizeof(double2);
+  if (xprod_uses_maps(g) != d.maps) return cudaErrorInvalidValue;
   const dim3 grid(g.ny / 2, g.nzd);
-#define HST_XPROD(NT, PPT)                                                                           \
-  {                                                                                                  \
-    big_smem(k_xprod<NT, PPT>);                                                                      \
-    k_xprod<NT, PPT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Z, d.Pp, d.twx, d.dyl, ph,      \
-                                                                 want_cfl, d.cfl);                   \
+#define HST_XPROD(NT, PPT)                                                                                   \
+  {                                                                                                          \
+    big_smem(k_xprod<NT, PPT>);                                                                              \
+    k_xprod<NT, PPT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Z, d.Pp, d.twx, d.dyl, ph, want_cfl,    \
+                                                                 d.cfl, d.tmZ, d.tmPp, d.err);               \
   }
-  HST_FFT_DISPATCH(NX, pts, HST_XPROD);
+  HST_FFT_DISPATCH(NX, pts, g.pptx == 8, HST_XPROD);
 #undef HST_XPROD
   return cudaGetLastError();
 }

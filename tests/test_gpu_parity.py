@@ -157,6 +157,25 @@ def test_c1_parity(variant):
     s.close()
 
 
+@pytest.mark.parametrize("ppt", [(8, 8), (16, 16), (8, 16)])
+def test_transform_plans_parity(monkeypatch, ppt):
+    """Both FFT plan families of the x and z kernels (8 points a thread with
+    the TMA-fed x kernel; 16 points a thread) on a 192 x 192 dealiased x 32
+    deck (nx = 63, nz = 64): 10 substeps against the oracle <= 1e-12, and
+    the CFL number of the last step."""
+    monkeypatch.setenv("HST_FFT_PPT_X", str(ppt[0]))
+    monkeypatch.setenv("HST_FFT_PPT_Z", str(ppt[1]))
+    deck = c1_deck(nx=63, nz=64, ny=32)
+    V0 = seeded_field(deck, seed=3, k0=6.0, energy=0.1)
+    s, o = make_pair(deck, V0)
+    assert (s.nxd, s.nzd) == (96, 192)
+    Vg, Vo = run_pair(s, o, deck["deltat"], 10)
+    err = rel_l2(Vg, Vo)
+    assert err <= 1e-12, (ppt, err)
+    assert abs(s.cfl - oracle.lib().ora_get_cfl(o.h)) <= 1e-12 * s.cfl
+    s.close()
+
+
 def test_cfl_matches_oracle():
     deck = c1_deck()
     V0 = seeded_field(deck)
