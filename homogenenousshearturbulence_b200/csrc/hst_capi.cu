@@ -453,7 +453,7 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   ok = ok && alloc((void**)&d.y, sizeof(double) * (ny + 4));
   ok = ok && alloc((void**)&d.dyl, sizeof(double) * ny);
   ok = ok && alloc((void**)&d.gdamp, sizeof(double) * g.ncol);
-  ok = ok && alloc((void**)&d.twx, sizeof(double2) * 2 * g.nxd);
+  ok = ok && alloc((void**)&d.twx, sizeof(double2) * 4 * g.nxd);
   ok = ok && alloc((void**)&d.twz, sizeof(double2) * g.nzd);
   // two words: the CFL maximum and the bounded-wait error flag
   ok = ok && alloc((void**)&d.cfl, 2 * sizeof(unsigned long long));
@@ -482,6 +482,8 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   cudaMemcpy(d.y, ctx->y.data(), sizeof(double) * (ny + 4), cudaMemcpyHostToDevice);
   cudaMemcpy(d.dyl, ctx->dyl.data(), sizeof(double) * ny, cudaMemcpyHostToDevice);
   cudaMemcpy(d.gdamp, ctx->gdamp.data(), sizeof(double) * g.ncol, cudaMemcpyHostToDevice);
+  tx.resize((size_t)4 * g.nxd, make_double2(0.0, 0.0));
+  hst::staged_twiddles(2 * g.nxd, tx.data() + 2 * g.nxd);
   cudaMemcpy(d.twx, tx.data(), sizeof(double2) * tx.size(), cudaMemcpyHostToDevice);
   cudaMemcpy(d.twz, tz.data(), sizeof(double2) * tz.size(), cudaMemcpyHostToDevice);
   cudaError_t e = hst::set_fft_constants();

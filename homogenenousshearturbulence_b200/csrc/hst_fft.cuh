@@ -167,6 +167,9 @@ __host__ __device__ constexpr int ls_padded(int N) { return N + N / 8 + 1; }
 // j = b / nl.  Inputs ld(l, j + r N/R), outputs st(l, (j/Ns) Ns R + j%Ns + r Ns).
 // SYNC: the stage reads and writes the same shared lines (all reads, then
 // a barrier, then all writes).
+// JF also selects the staged twiddle table: tw points at this stage's
+// block [r - 1][kk] of W^(kk r N/(Ns R)), r = 1..R-1, kk = 0..Ns-1, so that
+// a warp's twiddle loads are contiguous.
 template <int R, int S, int PPT, bool SYNC, typename LD, typename ST, bool JF = false>
 __device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const cxd* __restrict__ tw, const LD& ld,
                                              const ST& st) {
@@ -187,7 +190,7 @@ __device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const cxd* _
       for (int r = 0; r < R; ++r) {
         cxd x = ld(l, j + r * nb);
         if (r > 0 && kk > 0) {
-          cxd w = __ldg(tw + kk * r * tstride);
+          cxd w = JF ? __ldg(tw + (r - 1) * Ns + kk) : __ldg(tw + kk * r * tstride);
           if (S > 0) w.y = -w.y;
           x = cmul(x, w);
         }
@@ -294,11 +297,13 @@ __device__ __forceinline__ void fft_fixed(int nl, const cxd* __restrict__ tw, cx
     __syncthreads();
     fft_stage_io<PL::r1, S, PPT, DST_SH, LT, ST, JF>(N, nl, PL::r0, tw, L, dst);
   } else {
+    // staged table (JF): stage 2's block first, then stage 3's
+    const cxd* tw3 = JF ? tw + (PL::r1 - 1) * PL::r0 : tw;
     fft_stage_io<PL::r0, S, PPT, SRC_SH, LD, LT, JF>(N, nl, 1, tw, src, L);
     __syncthreads();
     fft_stage_io<PL::r1, S, PPT, true, LT, LT, JF>(N, nl, PL::r0, tw, L, L);
     __syncthreads();
-    fft_stage_io<PL::r2, S, PPT, DST_SH, LT, ST, JF>(N, nl, PL::r0 * PL::r1, tw, L, dst);
+    fft_stage_io<PL::r2, S, PPT, DST_SH, LT, ST, JF>(N, nl, PL::r0 * PL::r1, tw3, L, dst);
   }
 }
 

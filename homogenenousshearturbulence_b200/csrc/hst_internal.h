@@ -31,7 +31,7 @@ struct DeviceState {
   double* y;            // y(-2:ny+1)
   double* dyl;          // dyl(0:ny-1)
   double* gdamp;        // gdamp(-nz:nz, 0:nx)
-  double2* twx;         // exp(-2 pi i e / (2 nxd))
+  double2* twx;         // exp(-2 pi i e / (2 nxd)), then the staged table of the x kernel's 8-point plan
   double2* twz;         // exp(-2 pi i e / nzd)
   unsigned long long* cfl;  // running max (bits of a non-negative double)
   int* err;                 // set by a kernel whose bounded wait ran out
@@ -70,6 +70,9 @@ cudaError_t launch_fill_ghosts(const Geometry& g, const DeviceState& d, const Ph
 size_t column_smem_bytes(const Geometry& g, int exact);
 // the TMA maps of Z and Pp for the x kernel (d.maps false when not used)
 cudaError_t make_transform_maps(const Geometry& g, DeviceState& d);
+// the stage-ordered twiddles of the 8-point plan of N into out (at most N
+// entries); returns their number, 0 for a length without such a plan
+int staged_twiddles(int N, double2* out);
 // the constant twiddles of the register DFTs, once per device
 cudaError_t set_fft_constants();
 // a transform length the FFT kernels support

@@ -303,10 +303,13 @@ __global__ void k_fill_ghosts(Geometry g, PhysScalars ps, double2* __restrict__ 
 constexpr int RT_W = 36;                                 // window rows
 constexpr int RT_STAGE = 3 * RT_W + 6 * RT_W + 2 * 32;  // double2 per stage: V[3][36], Q[6][36], old[2][32]
 constexpr int RT_WARPS = 4;
+#ifndef RT_MINB
+#define RT_MINB 4  // 128 registers: four 4-warp blocks an SM (0.52 against 0.69 ms at 384^2 x 256)
+#endif
 constexpr int RT_WAIT_LIMIT = 1 << 22;
 
 template <bool EXACT, bool NONLIN>
-__global__ void __launch_bounds__(32 * RT_WARPS) k_rhs_tiled(ColumnArgs a, int* __restrict__ err) {
+__global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs a, int* __restrict__ err) {
   extern __shared__ __align__(128) double2 smt[];
   __shared__ __align__(8) uint64_t bars[RT_WARPS][2];
   const Geometry& g = a.g;

@@ -14,6 +14,8 @@
 // products).  Z and Pp are stored [component][y tile][kz][ix][Ty]: a block
 // of k_zinv / k_zfwd (one x mode, one y tile, all kz) then spans a few
 // huge pages instead of one page per kz.
+#include <cmath>
+
 #include "hst_dev.cuh"
 #include "hst_fft.cuh"
 #include "hst_internal.h"
@@ -231,7 +233,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
     __syncthreads();
     if (!tile_ok) return;
     const XinvSh xs = {stg, nxB, nx, NX};
-    fft_sel<NT, +1, PPT, false, true, JF>(NX, 3, twx, sh, xs, L);
+    fft_sel<NT, +1, PPT, false, true, JF>(NX, 3, twx + NX, sh, xs, L);
   } else {
     const XinvSrc xs = {Z + tile + yi0, cs, Ty, nx, NX};
     fft_sel<NT, +1, PPT, false, true, JF>(NX, 3, twx, sh, xs, L);
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   }
   // the six product lines, transformed forward in place
   const ProdSrc<LT> ps6 = {L, ps.factor};
-  fft_sel<NT, -1, PPT, true, true, JF>(NX, 6, twx, sh, ps6, L);
+  fft_sel<NT, -1, PPT, true, true, JF>(NX, 6, JF ? twx + NX : twx, sh, ps6, L);
   __syncthreads();
   // separate the two real transforms of each line, keep kx = 0..nx
   for (int e = threadIdx.x; e < nxB * 3; e += blockDim.x) {
@@ -282,6 +284,37 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
       bulk_wait_read_all();
     }
   }
+}
+
+// ------------------------------------------------------- staged twiddles ----
+// The twiddles of the 8-point plan of N in stage order (see fft_stage_io):
+// for each stage after the first, [r - 1][kk] = W_N^(kk r N/(Ns R)).
+template <int N>
+static int staged_twiddles_t(double2* out) {
+  using PL = Plan8<N>;
+  const int rad[3] = {PL::r0, PL::r1, PL::r2};
+  int n = 0, Ns = 1;
+  for (int st = 0; st < PL::n; ++st) {
+    const int R = rad[st];
+    if (Ns > 1)
+      for (int r = 1; r < R; ++r)
+        for (int kk = 0; kk < Ns; ++kk) {
+          const long e = (long)kk * r * (N / (Ns * R)) % N;
+          long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)e / (long double)N;
+          out[n++] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+    Ns *= R;
+  }
+  return n;
+}
+
+int staged_twiddles(int N, double2* out) {
+  switch (N) {
+    case 192: return staged_twiddles_t<192>(out);
+    case 384: return staged_twiddles_t<384>(out);
+    case 768: return staged_twiddles_t<768>(out);
+  }
+  return 0;
 }
 
 // ------------------------------------------------------------- TMA maps ----
