@@ -303,6 +303,10 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
   g.P = P;
   g.m = p.ny / P;
   g.MS = g.m | 1;
+  if (hst::column_smem_bytes(g, 1) > 200 * 1024) {
+    why = "ny too large for one line-solver group's shared memory";
+    return HST_EARG;
+  }
   // FFT points per thread: 8 selects the low-register plans (lengths 192,
   // 384, 768; the x kernel then moves its tiles by TMA).  Measured at
   // 384^2 x 256: x 8 (1.31 against 2.41 ms), z 16 (0.26/0.50 against

@@ -206,6 +206,7 @@ __global__ void k_column(ColumnArgs a) {
   group_solve<P>(K_DY, 0.0, ni, kk, thn, DS, G, bufB, fac, s, gmask);
   __syncwarp(gmask);
   // u, w from eta and dv/dy, into bufA (u) and bufB (w)
+  const double rkk = c00 ? 0.0 : 1.0 / kk;
   for (int r = s; r < ny; r += P) {
     cxd eta = bufA[G.at(r)], dv = bufB[G.at(r)];
     cxd u, w;
@@ -214,8 +215,8 @@ __global__ void k_column(ColumnArgs a) {
       w = mkc(eta.y, 0.0);
     } else {
       // (i alfa dv - i beta eta) / k2, (i beta dv + i alfa eta) / k2
-      u = mkc((-al * dv.y + be * eta.y) / kk, (al * dv.x - be * eta.x) / kk);
-      w = mkc((-be * dv.y - al * eta.y) / kk, (be * dv.x + al * eta.x) / kk);
+      u = mkc((-al * dv.y + be * eta.y) * rkk, (al * dv.x - be * eta.x) * rkk);
+      w = mkc((-be * dv.y - al * eta.y) * rkk, (be * dv.x + al * eta.x) * rkk);
     }
     bufA[G.at(r)] = u;
     bufB[G.at(r)] = w;
@@ -412,10 +413,14 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
     k_column<32, EXACT, NONLIN, COL_RHS><<<blocks, 128, 0, st>>>(a);
     return cudaGetLastError();
   }
-  int T = P >= 32 ? 32 : 64;
-  if (T < P) T = P;
-  int groups = T / P;
-  size_t smem = column_smem_bytes(g, EXACT) * groups;
+  // 32 or 64 threads, fewer groups when their shared memory would not fit
+  const size_t per = column_smem_bytes(g, EXACT);
+  int groups = (P >= 32 ? 32 : 64) / P;
+  if (groups < 1) groups = 1;
+  while (groups > 1 && per * groups > 200 * 1024) groups >>= 1;
+  if (per * groups > 200 * 1024) return cudaErrorInvalidValue;
+  const int T = groups * P;
+  size_t smem = per * groups;
   cudaFuncSetAttribute(k_column<P, EXACT, NONLIN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   int blocks = (g.ncol + groups - 1) / groups;
   k_column<P, EXACT, NONLIN, MODE><<<blocks, T, smem, st>>>(a);
@@ -472,10 +477,12 @@ cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysSca
 template <int P>
 static cudaError_t launch_line_solve_t(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int sys,
                                        double lambda, int src, int dst, double sx, double sz, cudaStream_t st) {
-  int T = P >= 32 ? 32 : 64;
-  if (T < P) T = P;
-  int groups = T / P;
   size_t per = ((size_t)P * g.MS * 2 + (size_t)(g.m - 2) * 4 * P) * sizeof(double);
+  int groups = (P >= 32 ? 32 : 64) / P;
+  if (groups < 1) groups = 1;
+  while (groups > 1 && per * groups > 200 * 1024) groups >>= 1;
+  if (per * groups > 200 * 1024) return cudaErrorInvalidValue;
+  const int T = groups * P;
   cudaFuncSetAttribute(k_line_solve<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   int blocks = (g.ncol + groups - 1) / groups;
   k_line_solve<P><<<blocks, T, per * groups, st>>>(g, ph, sys, lambda, d.F[src], d.F[dst], sx, sz, d.der, d.derS);
