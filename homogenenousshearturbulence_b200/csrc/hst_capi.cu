@@ -150,6 +150,12 @@ struct hst_ctx {
   std::vector<int> ev_class;  // class of each recorded pair
   double prof_ms[HST_KC_N];
   long long prof_n[HST_KC_N];
+  // asynchronous host I/O of V1..V3 (hst_gpu_upload_async and friends): a
+  // copy-in and a copy-out stream, and a device snapshot of each component
+  // that the copy-out stream reads while the solver goes on
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t ev_main = nullptr, ev_in = nullptr, ev_stage = nullptr, ev_out = nullptr;
+  double2* snap[3] = {nullptr, nullptr, nullptr};
 };
 
 // Runs `launch` (which queues one kernel on ctx->stream) between two events
@@ -508,6 +514,15 @@ extern "C" int hst_gpu_destroy(hst_ctx* ctx) {
   if (!ctx) return HST_EARG;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (cudaStream_t q : {ctx->s_in, ctx->s_out})
+    if (q) {
+      cudaStreamSynchronize(q);
+      cudaStreamDestroy(q);
+    }
+  for (cudaEvent_t e : {ctx->ev_main, ctx->ev_in, ctx->ev_stage, ctx->ev_out})
+    if (e) cudaEventDestroy(e);
+  for (double2* q : ctx->snap)
+    if (q) cudaFree(q);
   for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
   free_device(ctx);
   if (ctx->h_gdamp) cudaFreeHost(ctx->h_gdamp);
@@ -565,6 +580,67 @@ extern "C" int hst_gpu_download(hst_ctx* ctx, int field, double* host) {
   CK(cudaSetDevice(ctx->device));
   CK(cudaMemcpyAsync(host, ctx->d.F[field], sizeof(double2) * ctx->g.nf, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  return HST_OK;
+}
+
+// ------------------------------------------------- asynchronous host I/O ----
+static int ensure_io(hst_ctx* ctx) {
+  if (ctx->s_in) return HST_OK;
+  CK(cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&ctx->ev_main, &ctx->ev_in, &ctx->ev_stage, &ctx->ev_out})
+    CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_upload_async(hst_ctx* ctx, int field, const double* host) {
+  if (!ctx || field < 0 || field > 2 || !host) return fail(ctx, HST_EARG, "upload_async: bad field %d", field);
+  CK(cudaSetDevice(ctx->device));
+  int rc = ensure_io(ctx);
+  if (rc != HST_OK) return rc;
+  // after everything queued so far on the solver's stream (the snapshot
+  // copies of earlier downloads included), before anything queued later
+  CK(cudaEventRecord(ctx->ev_main, ctx->stream));
+  CK(cudaStreamWaitEvent(ctx->s_in, ctx->ev_main, 0));
+  CK(cudaMemcpyAsync(ctx->d.F[field], host, sizeof(double2) * ctx->g.nf, cudaMemcpyHostToDevice, ctx->s_in));
+  CK(cudaEventRecord(ctx->ev_in, ctx->s_in));
+  CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_in, 0));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_download_async(hst_ctx* ctx, int field, double* host) {
+  if (!ctx || field < 0 || field > 2 || !host) return fail(ctx, HST_EARG, "download_async: bad field %d", field);
+  CK(cudaSetDevice(ctx->device));
+  int rc = ensure_io(ctx);
+  if (rc != HST_OK) return rc;
+  const size_t bytes = sizeof(double2) * ctx->g.nf;
+  if (!ctx->snap[field] && cudaMalloc((void**)&ctx->snap[field], bytes) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->snap[field] = nullptr;
+    return fail(ctx, HST_ENOMEM, "download_async: snapshot of %.2f GB refused", bytes / 1e9);
+  }
+  // the snapshot may be overwritten once the previous copy-out has read it
+  CK(cudaEventRecord(ctx->ev_out, ctx->s_out));
+  CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_out, 0));
+  CK(cudaMemcpyAsync(ctx->snap[field], ctx->d.F[field], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaEventRecord(ctx->ev_stage, ctx->stream));
+  CK(cudaStreamWaitEvent(ctx->s_out, ctx->ev_stage, 0));
+  CK(cudaMemcpyAsync(host, ctx->snap[field], bytes, cudaMemcpyDeviceToHost, ctx->s_out));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_wait_io(hst_ctx* ctx) {
+  if (!ctx) return HST_EARG;
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->s_in) return HST_OK;
+  // the solver's stream also waits for both copy streams, so that work
+  // queued on it afterwards (or an event recorded there) follows the copies
+  CK(cudaEventRecord(ctx->ev_in, ctx->s_in));
+  CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_in, 0));
+  CK(cudaEventRecord(ctx->ev_out, ctx->s_out));
+  CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_out, 0));
+  CK(cudaStreamSynchronize(ctx->s_in));
+  CK(cudaStreamSynchronize(ctx->s_out));
   return HST_OK;
 }
 

@@ -86,6 +86,9 @@ def lib():
             "hst_gpu_kernel_times": (i, [vp, P(d), P(ct.c_longlong)]),
             "hst_gpu_reset_kernel_times": (i, [vp]),
             "hst_gpu_stream": (vp, [vp]),
+            "hst_gpu_upload_async": (i, [vp, i, vp]),
+            "hst_gpu_download_async": (i, [vp, i, vp]),
+            "hst_gpu_wait_io": (i, [vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -344,6 +347,18 @@ class Solver:
     def download_ptr(self, field: int, ptr: int):
         self._check(lib().hst_gpu_download(self._h, field, ct.cast(ct.c_void_p(ptr), ct.POINTER(ct.c_double))),
                     "download")
+
+    def upload_async_ptr(self, field: int, ptr: int):
+        """queue the upload of V1..V3 from a pinned host address (see wait_io)"""
+        self._check(lib().hst_gpu_upload_async(self._h, field, ct.c_void_p(ptr)), "upload_async")
+
+    def download_async_ptr(self, field: int, ptr: int):
+        """queue the download of V1..V3 as it is now into a pinned host address"""
+        self._check(lib().hst_gpu_download_async(self._h, field, ct.c_void_p(ptr)), "download_async")
+
+    def wait_io(self):
+        """wait for every queued asynchronous upload and download"""
+        self._check(lib().hst_gpu_wait_io(self._h), "wait_io")
 
     @property
     def launches(self) -> int:

@@ -104,6 +104,25 @@ int hst_gpu_get_tables(const hst_ctx* ctx, double* der, double* y, double* dyl);
 int hst_gpu_upload(hst_ctx* ctx, int field, const double* host);
 int hst_gpu_download(hst_ctx* ctx, int field, double* host);
 
+/* Asynchronous host I/O of the velocity components (field HST_V1..HST_V3),
+ * for a driver that overlaps the two copy directions with each other and
+ * with the solver.  No counterpart in the reference, whose target updates
+ * (src/hst.f90:76,110,121,141) are synchronous.
+ *   upload_async:   the host buffer (pinned: cudaHostAlloc / registered)
+ *                   is copied in on a copy-in stream after all work queued
+ *                   so far; work queued later waits for it.  The buffer must
+ *                   not change until hst_gpu_wait_io.
+ *   download_async: the field as it is at this point of the queue (a
+ *                   device snapshot, taken on the solver's stream) is copied
+ *                   out on a copy-out stream; the host buffer is valid after
+ *                   hst_gpu_wait_io.  The first call per component allocates
+ *                   its snapshot.
+ *   wait_io:        the host waits for every asynchronous copy; work queued
+ *                   afterwards follows them. */
+int hst_gpu_upload_async(hst_ctx* ctx, int field, const double* host);
+int hst_gpu_download_async(hst_ctx* ctx, int field, double* host);
+int hst_gpu_wait_io(hst_ctx* ctx);
+
 /* ------------------------------------------------------------------- path */
 /* timestep() (src/hst_equations.f90:56-87): three substeps; *time is
  * advanced as the reference advances it; *cfl receives the CFL number of
