@@ -176,6 +176,20 @@ def test_transform_plans_parity(monkeypatch, ppt):
     s.close()
 
 
+@pytest.mark.parametrize("ny,exact", [(256, False), (256, True), (512, False), (512, True)])
+def test_column_tall_lines_parity(ny, exact):
+    """The column kernel with 8 and 16 rows per lane of a 32-lane solver
+    group (ny = 256, 512; the sizes of the 384^2 and 768^2 workloads) on a
+    narrow deck (nx = 15, nz = 16): 10 substeps against the oracle <= 1e-12."""
+    deck = c1_deck(nx=15, nz=16, ny=ny, exact_shift=exact)
+    V0 = seeded_field(deck, seed=9, k0=4.0, energy=0.1)
+    s, o = make_pair(deck, V0)
+    Vg, Vo = run_pair(s, o, deck["deltat"], 10)
+    err = rel_l2(Vg, Vo)
+    assert err <= 1e-12, (ny, exact, err)
+    s.close()
+
+
 def test_cfl_matches_oracle():
     deck = c1_deck()
     V0 = seeded_field(deck)
