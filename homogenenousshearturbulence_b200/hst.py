@@ -107,6 +107,9 @@ DECK_DEFAULTS = dict(  # src/hst_input.f90:140-155
     amplitude=1.0e-3, seed=1, kpeak=4.0,
     damp_kpar=0.0, damp_kperp=0.0, damp_rate=0.0, damp_hard=False, damp_edge=0.0, damp_norm=2.0,
     damp_mean=False, damp_follow=True, damp_angle=0.0,
+    # the Stokes-layer forcing (src/hst_input.f90, &physics sl_*): read so
+    # that a deck using it is refused, not run without it
+    sl_amplitude=0.0, sl_period=0.0, sl_delta=0.0, sl_start=0.0, sl_bodyforce=False, sl_ramp=False,
 )
 
 
@@ -179,6 +182,8 @@ class Solver:
         if deck:
             cfg.update(deck)
         cfg.update(kw)
+        if float(cfg.get("sl_amplitude", 0.0)) != 0.0:
+            raise HstError("the Stokes-layer forcing (sl_amplitude != 0) is not part of the GPU substep")
         self.cfg = cfg
         p = Params()
         p.nx, p.ny, p.nz = int(cfg["nx"]), int(cfg["ny"]), int(cfg["nz"])

@@ -57,3 +57,28 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(hst, "_lib", None)
     with pytest.raises(hst.HstError):
         hst.lib()
+
+
+def test_stokes_layer_deck_is_refused(golden):
+    """The Stokes-layer forcing is outside the GPU substep: a deck that uses
+    it is refused (HstError) before any device work, not run without it."""
+    deck = hst.read_deck(golden / "small_stokes.in")
+    assert deck["sl_amplitude"] == 0.5
+    with pytest.raises(hst.HstError):
+        hst.Solver(deck)
+
+
+def test_async_io_and_noalloc_reject_bad_arguments():
+    L = hst.lib()
+    assert L.hst_gpu_upload_async(None, 0, None) == -1
+    assert L.hst_gpu_download_async(None, 0, None) == -1
+    assert L.hst_gpu_wait_io(None) == -1
+    f = L.hst_gpu_line_solve_noalloc
+    d, i, vp = ct.c_double, ct.c_int, ct.c_void_p
+    f.restype = i
+    f.argtypes = [i, i, i, d, d, d, i, d, vp, vp, vp, d, d, vp, ct.c_char_p, i]
+    msg = ct.create_string_buffer(128)
+    # sizes are checked before any CUDA call
+    assert f(15, 4096, 15, 1.0, 1.0, 100.0, 1, 1.0, 16, 32, 64, 0.0, 0.0, None, msg, 128) == -1
+    assert b"scratch" in msg.value
+    assert f(15, 31, 15, 1.0, 1.0, 100.0, 1, 1.0, 16, 32, 64, 0.0, 0.0, None, msg, 128) == -1
