@@ -63,24 +63,28 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def alg_bytes(deck, nxd, nzd, split):
-    """Compulsory HBM bytes per launch of each kernel and per substep (FP64).
+def alg_bytes(deck, nxd, nzd, split, mixed=False):
+    """Compulsory HBM bytes per launch of each kernel and per substep.
     Ns = ny (2nz+1)(nx+1) spectral points per component, Nzx = ny nzd (nx+1).
     With the column stage split, `rhs` streams V, Q, old in and old, rhs out
     (15 Ns) and `column` reads rhs and writes V (5 Ns; 9 Ns with exact_shift,
-    which re-reads and rewrites old); fused, `column` moves 16 Ns."""
+    which re-reads and rewrites old); fused, `column` moves 16 Ns.  The
+    substep figure is the four-pass model 16 (25 Ns + 18 Nzx).  Mixed
+    precision: Z, Pp and Q are 8-byte complex64, V, old and rhs stay 16-byte
+    complex128; the substep model becomes 16 13 Ns + 8 (12 Ns + 18 Nzx)."""
     nx, ny, nz = deck["nx"], deck["ny"], deck["nz"]
     Ns = ny * (2 * nz + 1) * (nx + 1)
     Nzx = ny * nzd * (nx + 1)
-    b = 16.0
+    b, t = 16.0, (8.0 if mixed else 16.0)
     k = {
-        "zinv": b * (3 * Ns + 3 * Nzx),
-        "xprod": b * (3 * Nzx + 6 * Nzx),
-        "zfwd": b * (6 * Nzx + 6 * Ns),
-        "rhs": b * (15 * Ns),
-        "column": b * ((9 if deck.get("exact_shift") else 5) * Ns if split else 16 * Ns),
+        "zinv": b * 3 * Ns + t * 3 * Nzx,
+        "xprod": t * (3 * Nzx + 6 * Nzx),
+        "zfwd": t * (6 * Nzx + 6 * Ns),
+        "rhs": b * 9 * Ns + t * 6 * Ns,
+        "column": b * ((9 if deck.get("exact_shift") else 5) * Ns if split else 10 * Ns) + (0 if split else t * 6 * Ns),
     }
-    return k, b * (25 * Ns + 18 * Nzx), Ns, Nzx
+    sub = b * 13 * Ns + t * (12 * Ns + 18 * Nzx)
+    return k, sub, Ns, Nzx
 
 
 class ClockSampler:
@@ -198,6 +202,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -233,8 +238,23 @@ def main():
     torch.cuda.set_device(dev)
     deck = dict(cfg["deck"])
     dt = deck["deltat"]
-    s = hst.Solver(deck, device=dev)
+    mixed = args.precision == "mixed"
+    s = hst.Solver(dict(deck, precision=args.precision), device=dev)
     V0 = seeded_field(cfg, s.y)
+    accuracy = None
+    if mixed:
+        # the error of the mixed-precision form against the FP64 form after
+        # 30 substeps from the same field, on this GPU
+        ref = hst.Solver(deck, device=dev)
+        for x in (s, ref):
+            x.time = 0.0
+            x.set_velocity(V0)
+            x.timesteps(10, dt)
+        va, vb = s.velocity(), ref.velocity()
+        num = np.linalg.norm((va - vb)[..., 2:-2])
+        den = np.linalg.norm(vb[..., 2:-2])
+        accuracy = {"rel_l2_vs_fp64": float(num / den), "substeps": 30}
+        ref.close()
     s.time = 0.0
     s.set_velocity(V0)
     stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", dev))
@@ -313,7 +333,7 @@ def main():
                "d2h_bytes_per_step": 3 * nbytes + 8, "steps": ke}
 
     if rank == 0:
-        per_kernel, b_sub, Ns, Nzx = alg_bytes(deck, s.nxd, s.nzd, ktimes.get("rhs", (0, 0))[1] > 0)
+        per_kernel, b_sub, Ns, Nzx = alg_bytes(deck, s.nxd, s.nzd, ktimes.get("rhs", (0, 0))[1] > 0, mixed)
         peak, peak_kind = peaks()
         kt = {k: v for k, v in ktimes.items() if v[1] > 0}
         top = max(kt, key=lambda k: kt[k][0])
@@ -321,14 +341,17 @@ def main():
         achieved = per_kernel[top] / (avg_ms / 1000.0) / 1e9
         traffic = None
         tf = ROOT / "profiles" / f"traffic_{args.config}.json"
-        if tf.exists():
+        if tf.exists() and not mixed:
             traffic = json.loads(tf.read_text()).get(top)
         sub_ms = ms / nsub
         line = {
             "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg["label"], "step": "one RK3 time step = 3 substeps (hst_gpu_timestep)",
+            "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
+            "config": {"workload": cfg["label"] + (", mixed precision (FP32 transforms, products and spectra; "
+                                                   "FP64 right-hand sides, shift and solves)" if mixed else ""),
+                       "precision": args.precision,
+                       "step": "one RK3 time step = 3 substeps (hst_gpu_timestep)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single field, 1 GPU",
                        "l2": "inputs larger than L2 (no flush)", "nxd": s.nxd, "nzd": s.nzd,
                        },
@@ -345,6 +368,8 @@ def main():
         }
         if e2e:
             line["e2e"] = e2e
+        if accuracy:
+            line["accuracy"] = accuracy
         if world == 1 and not args.no_cpu_baseline:
             rate, n, threads, w = cpu_oracle_rate(cfg, 2, budget_s=20.0)
             line["cpu_baseline"] = {"value": rate, "unit": unit, "cores": threads, "kind": "port",

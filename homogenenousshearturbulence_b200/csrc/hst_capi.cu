@@ -325,6 +325,21 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
   };
   g.pptx = ppt_of("HST_FFT_PPT_X", 8);
   g.pptz = ppt_of("HST_FFT_PPT_Z", g.nzd >= 768 ? 8 : 16);
+  // mixed precision: the FP32 transforms of the lengths it compiles
+  // (8 points a thread, 16 at 96) and the streamed right-hand sides
+  g.mp = p.precision == HST_PREC_MIXED;
+  if (p.precision != HST_PREC_FP64 && p.precision != HST_PREC_MIXED) {
+    why = "precision must be HST_PREC_FP64 or HST_PREC_MIXED";
+    return HST_EARG;
+  }
+  if (g.mp) {
+    if (!hst::mp_length_ok(2 * g.nxd) || !hst::mp_length_ok(g.nzd) || p.ny % 32 != 0) {
+      why = "mixed precision needs 2 nxd and nzd in {96, 192, 384, 768} and ny a multiple of 32";
+      return HST_EARG;
+    }
+    g.pptx = 8;
+    g.pptz = g.nzd == 96 ? 16 : 8;
+  }
   // transform y tile (at most 512 threads for the 8-point z plans)
   g.Ty = 2;
   for (int t : {8, 4}) {
@@ -344,7 +359,7 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
 static double dev_bytes(const Geometry& g) {
   double nf = (double)g.nf;
   double z = 3.0 * g.nzd * g.ny * g.nxB, pp = 6.0 * g.nzd * g.ny * g.nxB, q = 6.0 * g.ncol * g.ny;
-  return 16.0 * (7.0 * nf + z + pp + q) + 8.0 * (20.0 * g.ny + 2.0 * g.ny + 4 + g.ncol);
+  return 16.0 * 7.0 * nf + (g.mp ? 8.0 : 16.0) * (z + pp + q) + 8.0 * (20.0 * g.ny + 2.0 * g.ny + 4 + g.ncol);
 }
 
 extern "C" double hst_gpu_device_bytes(const hst_gpu_params* p) {
@@ -378,7 +393,7 @@ static void free_device(hst_ctx* c) {
   DeviceState& d = c->d;
   for (int i = 0; i < 7; ++i)
     if (d.F[i]) cudaFree(d.F[i]);
-  void* ps[] = {d.Z, d.Pp, d.Q, d.der, d.derS, d.y, d.dyl, d.gdamp, d.twx, d.twz, d.cfl};
+  void* ps[] = {d.Z, d.Pp, d.Q, d.der, d.derS, d.y, d.dyl, d.gdamp, d.twx, d.twz, d.twxf, d.twzf, d.cfl};
   for (void* q : ps)
     if (q) cudaFree(q);
   std::memset(&d, 0, sizeof d);
@@ -413,6 +428,16 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   }
   ctx->p.nxd = ctx->g.nxd;
   ctx->p.nzd = ctx->g.nzd;
+  if (ctx->g.mp) {
+    // the FP32 product spectra are read only by the streamed right-hand-side kernel
+    const char* t = std::getenv("HST_RHS_TILED");
+    if (!ctx->column_split || (t && std::atoi(t) == 0)) {
+      std::fprintf(stderr, "hst_gpu_create: mixed precision needs the split column stage and the streamed "
+                           "right-hand sides (HST_COLUMN_FUSED, HST_RHS_TILED unset)\n");
+      delete ctx;
+      return HST_EARG;
+    }
+  }
   const hst_gpu_params& p = ctx->p;
   const Geometry& g = ctx->g;
   ctx->device = p.device;
@@ -455,9 +480,10 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   DeviceState& d = ctx->d;
   bool ok = true;
   for (int i = 0; i < 7 && ok; ++i) ok = alloc((void**)&d.F[i], sizeof(double2) * g.nf);
-  ok = ok && alloc((void**)&d.Z, sizeof(double2) * 3 * (size_t)g.nzd * g.ny * g.nxB);
-  ok = ok && alloc((void**)&d.Pp, sizeof(double2) * 6 * (size_t)g.nzd * g.ny * g.nxB);
-  ok = ok && alloc((void**)&d.Q, sizeof(double2) * 6 * (size_t)g.ncol * g.ny);
+  const size_t es = g.mp ? sizeof(float2) : sizeof(double2);  // the transforms' complex element
+  ok = ok && alloc((void**)&d.Z, es * 3 * (size_t)g.nzd * g.ny * g.nxB);
+  ok = ok && alloc((void**)&d.Pp, es * 6 * (size_t)g.nzd * g.ny * g.nxB);
+  ok = ok && alloc((void**)&d.Q, es * 6 * (size_t)g.ncol * g.ny);
   ok = ok && alloc((void**)&d.der, sizeof(double) * 20 * (size_t)ny);
   ok = ok && alloc((void**)&d.derS, sizeof(double) * 20 * (size_t)ny);
   ok = ok && alloc((void**)&d.y, sizeof(double) * (ny + 4));
@@ -465,6 +491,8 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   ok = ok && alloc((void**)&d.gdamp, sizeof(double) * g.ncol);
   ok = ok && alloc((void**)&d.twx, sizeof(double2) * 4 * g.nxd);
   ok = ok && alloc((void**)&d.twz, sizeof(double2) * g.nzd);
+  ok = ok && alloc((void**)&d.twxf, sizeof(float2) * 4 * g.nxd);
+  ok = ok && alloc((void**)&d.twzf, sizeof(float2) * g.nzd);
   // two words: the CFL maximum and the bounded-wait error flag
   ok = ok && alloc((void**)&d.cfl, 2 * sizeof(unsigned long long));
   if (ok) d.err = reinterpret_cast<int*>(d.cfl + 1);
@@ -495,6 +523,21 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   tx.resize((size_t)4 * g.nxd, make_double2(0.0, 0.0));
   hst::staged_twiddles(2 * g.nxd, tx.data() + 2 * g.nxd);
   cudaMemcpy(d.twx, tx.data(), sizeof(double2) * tx.size(), cudaMemcpyHostToDevice);
+  {
+    // FP32 copies (rounded from the long double values)
+    std::vector<float2> fx((size_t)4 * g.nxd, make_float2(0.f, 0.f)), fz(g.nzd);
+    for (int k = 0; k < 2 * g.nxd; ++k) {
+      long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)(2 * g.nxd);
+      fx[k] = make_float2((float)cosl(a), (float)sinl(a));
+    }
+    hst::staged_twiddles(2 * g.nxd, fx.data() + 2 * g.nxd);
+    for (int k = 0; k < g.nzd; ++k) {
+      long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)g.nzd;
+      fz[k] = make_float2((float)cosl(a), (float)sinl(a));
+    }
+    cudaMemcpy(d.twxf, fx.data(), sizeof(float2) * fx.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(d.twzf, fz.data(), sizeof(float2) * fz.size(), cudaMemcpyHostToDevice);
+  }
   cudaMemcpy(d.twz, tz.data(), sizeof(double2) * tz.size(), cudaMemcpyHostToDevice);
   cudaError_t e = hst::set_fft_constants();
   if (e == cudaSuccess) e = hst::make_transform_maps(g, d);

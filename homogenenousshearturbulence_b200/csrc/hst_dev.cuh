@@ -36,6 +36,24 @@ __device__ __forceinline__ cxd cdiv(cxd a, cxd b) {
     return mkc((a.x * r + a.y) / d, (a.y * r - a.x) / d);
   }
 }
+// the same operations on complex64 (the transforms of the mixed-precision form)
+typedef float2 cxf;
+__device__ __forceinline__ cxf cadd(cxf a, cxf b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ cxf csub(cxf a, cxf b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ cxf cmul(cxf a, cxf b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ cxf cscale(float s, cxf a) { return make_float2(s * a.x, s * a.y); }
+__device__ __forceinline__ cxf cconj(cxf a) { return make_float2(a.x, -a.y); }
+// the real scalar type of a complex type
+template <typename C>
+struct RealOf;
+template <>
+struct RealOf<double2> {
+  typedef double T;
+};
+template <>
+struct RealOf<float2> {
+  typedef float T;
+};
 __device__ __forceinline__ double shfl_d(unsigned mask, double v, int src, int width) {
   return __shfl_sync(mask, v, src, width);
 }

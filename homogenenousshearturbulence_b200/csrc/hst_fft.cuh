@@ -25,26 +25,35 @@ namespace hst {
 
 #define HST_SQRT3_2 0.86602540378443864676
 
-// exp(-2 pi i k / 48), k = 0..47 (set per device by set_fft_constants;
-// this header is included by one translation unit only)
+// exp(-2 pi i k / 48), k = 0..47, in both precisions (set per device by
+// set_fft_constants; this header is included by one translation unit only)
 __constant__ double2 c_w48[48];
+__constant__ float2 c_w48f[48];
+template <typename C>
+__device__ __forceinline__ C w48(int i);
+template <>
+__device__ __forceinline__ double2 w48<double2>(int i) { return c_w48[i]; }
+template <>
+__device__ __forceinline__ float2 w48<float2>(int i) { return c_w48f[i]; }
 
 template <int R, int S>
 struct DFT;
 
 template <int S>
 struct DFT<2, S> {
-  static __device__ __forceinline__ void run(cxd* v) {
-    cxd a = v[0], b = v[1];
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) {
+    C a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   }
 };
 template <int S>
 struct DFT<4, S> {
-  static __device__ __forceinline__ void run(cxd* v) {
-    cxd a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]), a2 = cadd(v[1], v[3]), a3 = csub(v[1], v[3]);
-    cxd a3r = S < 0 ? mkc(a3.y, -a3.x) : mkc(-a3.y, a3.x);
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) {
+    C a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]), a2 = cadd(v[1], v[3]), a3 = csub(v[1], v[3]);
+    C a3r = S < 0 ? C{a3.y, -a3.x} : C{-a3.y, a3.x};
     v[0] = cadd(a0, a2);
     v[2] = csub(a0, a2);
     v[1] = cadd(a1, a3r);
@@ -53,10 +62,13 @@ struct DFT<4, S> {
 };
 template <int S>
 struct DFT<3, S> {
-  static __device__ __forceinline__ void run(cxd* v) {
-    cxd t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
-    cxd m = mkc(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-    cxd r = S < 0 ? mkc(HST_SQRT3_2 * t2.y, -HST_SQRT3_2 * t2.x) : mkc(-HST_SQRT3_2 * t2.y, HST_SQRT3_2 * t2.x);
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) {
+    typedef typename RealOf<C>::T T;
+    const T h = T(0.5), q = T(HST_SQRT3_2);
+    C t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+    C m = C{v[0].x - h * t1.x, v[0].y - h * t1.y};
+    C r = S < 0 ? C{q * t2.y, -q * t2.x} : C{-q * t2.y, q * t2.x};
     v[0] = cadd(v[0], t1);
     v[1] = cadd(m, r);
     v[2] = csub(m, r);
@@ -64,12 +76,12 @@ struct DFT<3, S> {
 };
 // R = A B: B DFTs of size A on the elements b + B a, the twiddles
 // W_R^(b ka), A DFTs of size B; output k = ka + A kb.
-template <int A, int B, int S>
-__device__ __forceinline__ void dft_ab(cxd* v) {
-  cxd o[A * B];
+template <int A, int B, int S, typename C>
+__device__ __forceinline__ void dft_ab(C* v) {
+  C o[A * B];
 #pragma unroll
   for (int b = 0; b < B; ++b) {
-    cxd t[A];
+    C t[A];
 #pragma unroll
     for (int a = 0; a < A; ++a) t[a] = v[b + B * a];
     DFT<A, S>::run(t);
@@ -78,7 +90,7 @@ __device__ __forceinline__ void dft_ab(cxd* v) {
       if (b * ka == 0) {
         v[b + B * ka] = t[ka];
       } else {
-        cxd w = c_w48[(b * ka * (48 / (A * B))) % 48];
+        C w = w48<C>((b * ka * (48 / (A * B))) % 48);
         if (S > 0) w.y = -w.y;
         v[b + B * ka] = cmul(t[ka], w);
       }
@@ -86,7 +98,7 @@ __device__ __forceinline__ void dft_ab(cxd* v) {
   }
 #pragma unroll
   for (int ka = 0; ka < A; ++ka) {
-    cxd t[B];
+    C t[B];
 #pragma unroll
     for (int b = 0; b < B; ++b) t[b] = v[b + B * ka];
     DFT<B, S>::run(t);
@@ -98,23 +110,28 @@ __device__ __forceinline__ void dft_ab(cxd* v) {
 }
 template <int S>
 struct DFT<6, S> {
-  static __device__ __forceinline__ void run(cxd* v) { dft_ab<3, 2, S>(v); }
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) { dft_ab<3, 2, S>(v); }
 };
 template <int S>
 struct DFT<8, S> {
-  static __device__ __forceinline__ void run(cxd* v) { dft_ab<4, 2, S>(v); }
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) { dft_ab<4, 2, S>(v); }
 };
 template <int S>
 struct DFT<12, S> {
-  static __device__ __forceinline__ void run(cxd* v) { dft_ab<4, 3, S>(v); }
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) { dft_ab<4, 3, S>(v); }
 };
 template <int S>
 struct DFT<16, S> {
-  static __device__ __forceinline__ void run(cxd* v) { dft_ab<4, 4, S>(v); }
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) { dft_ab<4, 4, S>(v); }
 };
 template <int S>
 struct DFT<24, S> {
-  static __device__ __forceinline__ void run(cxd* v) { dft_ab<8, 3, S>(v); }
+  template <typename C>
+  static __device__ __forceinline__ void run(C* v) { dft_ab<8, 3, S>(v); }
 };
 
 // The runtime radix plan of N: radix-16 stages while more than 24 is left,
@@ -146,21 +163,25 @@ __host__ inline bool plan_ok(int N) {
 }
 
 // Shared-memory line access (line stride LS)
-struct ShLines {
-  cxd* p;
+template <typename C>
+struct ShLinesT {
+  C* p;
   int LS;
-  __device__ __forceinline__ cxd operator()(int l, int i) const { return p[l * LS + i]; }
-  __device__ __forceinline__ void operator()(int l, int i, cxd v) const { p[l * LS + i] = v; }
+  __device__ __forceinline__ C operator()(int l, int i) const { return p[l * LS + i]; }
+  __device__ __forceinline__ void operator()(int l, int i, C v) const { p[l * LS + i] = v; }
 };
+typedef ShLinesT<cxd> ShLines;
 // The same with one pad element after every 8: with butterflies mapped
 // index-fastest (JF) the radix-8/6/12 exchanges of the 8-point plans are
 // then free of bank conflicts.  Line stride ls_padded(N).
-struct ShLinesP {
-  cxd* p;
+template <typename C>
+struct ShLinesPT {
+  C* p;
   int LS;
-  __device__ __forceinline__ cxd operator()(int l, int i) const { return p[l * LS + i + (i >> 3)]; }
-  __device__ __forceinline__ void operator()(int l, int i, cxd v) const { p[l * LS + i + (i >> 3)] = v; }
+  __device__ __forceinline__ C operator()(int l, int i) const { return p[l * LS + i + (i >> 3)]; }
+  __device__ __forceinline__ void operator()(int l, int i, C v) const { p[l * LS + i + (i >> 3)] = v; }
 };
+typedef ShLinesPT<cxd> ShLinesP;
 __host__ __device__ constexpr int ls_padded(int N) { return N + N / 8 + 1; }
 
 // One radix-R stage.  Butterfly b of the block: line l = b % nl, index
@@ -170,14 +191,14 @@ __host__ __device__ constexpr int ls_padded(int N) { return N + N / 8 + 1; }
 // JF also selects the staged twiddle table: tw points at this stage's
 // block [r - 1][kk] of W^(kk r N/(Ns R)), r = 1..R-1, kk = 0..Ns-1, so that
 // a warp's twiddle loads are contiguous.
-template <int R, int S, int PPT, bool SYNC, typename LD, typename ST, bool JF = false>
-__device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const cxd* __restrict__ tw, const LD& ld,
+template <int R, int S, int PPT, bool SYNC, typename LD, typename ST, bool JF = false, typename C = cxd>
+__device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const C* __restrict__ tw, const LD& ld,
                                              const ST& st) {
   constexpr int MAXB = (PPT + R - 1) / R;
   const int nb = N / R;
   const int total = nb * nl;
   const int tstride = N / (Ns * R);
-  cxd v[MAXB][R];
+  C v[MAXB][R];
   int lj[MAXB];
 #pragma unroll
   for (int k = 0; k < MAXB; ++k) {
@@ -188,9 +209,9 @@ __device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const cxd* _
       int kk = j % Ns;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        cxd x = ld(l, j + r * nb);
+        C x = ld(l, j + r * nb);
         if (r > 0 && kk > 0) {
-          cxd w = JF ? __ldg(tw + (r - 1) * Ns + kk) : __ldg(tw + kk * r * tstride);
+          C w = JF ? __ldg(tw + (r - 1) * Ns + kk) : __ldg(tw + kk * r * tstride);
           if (S > 0) w.y = -w.y;
           x = cmul(x, w);
         }
@@ -213,8 +234,8 @@ __device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const cxd* _
   }
 }
 
-template <int S, int PPT, bool SYNC, typename LD, typename ST>
-__device__ __forceinline__ void fft_stage_r(int R, int N, int nl, int Ns, const cxd* __restrict__ tw, const LD& ld,
+template <int S, int PPT, bool SYNC, typename LD, typename ST, typename C>
+__device__ __forceinline__ void fft_stage_r(int R, int N, int nl, int Ns, const C* __restrict__ tw, const LD& ld,
                                             const ST& st) {
   switch (R) {
     case 2: fft_stage_io<2, S, PPT, SYNC>(N, nl, Ns, tw, ld, st); break;
@@ -234,10 +255,10 @@ __device__ __forceinline__ void fft_stage_r(int R, int N, int nl, int Ns, const 
 // exchange through `sh` (nl lines of stride N+1).  SRC_SH / DST_SH: src
 // reads, dst writes the same shared buffer (the stage then synchronises
 // between its reads and its writes).  Requires nl N <= PPT blockDim.x.
-template <int S, int PPT, bool SRC_SH, bool DST_SH, typename LD, typename ST>
-__device__ void fft_global(int N, int nl, const cxd* __restrict__ tw, cxd* sh, const LD& src, const ST& dst) {
+template <int S, int PPT, bool SRC_SH, bool DST_SH, typename LD, typename ST, typename C>
+__device__ void fft_global(int N, int nl, const C* __restrict__ tw, C* sh, const LD& src, const ST& dst) {
   const FftPlan P = make_plan(N);
-  const ShLines L = {sh, N + 1};
+  const ShLinesT<C> L = {sh, N + 1};
   int Ns = 1;
   if (P.n == 1) {
     fft_stage_r<S, PPT, SRC_SH && DST_SH>(P.r[0], N, nl, Ns, tw, src, dst);
@@ -284,32 +305,32 @@ template <> struct Plan8<192> { static constexpr int n = 3, r0 = 8, r1 = 4, r2 =
 template <> struct Plan8<384> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 = 6; };
 template <> struct Plan8<768> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 = 12; };
 
-template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF, typename LD, typename ST>
-__device__ __forceinline__ void fft_fixed(int nl, const cxd* __restrict__ tw, cxd* sh, const LD& src, const ST& dst) {
+template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF, typename LD, typename ST, typename C>
+__device__ __forceinline__ void fft_fixed(int nl, const C* __restrict__ tw, C* sh, const LD& src, const ST& dst) {
   using PL = std::conditional_t<(PPT <= 8), Plan8<N>, Plan<N>>;
   static_assert(PL::n > 0, "no compile-time plan for this length and points per thread");
-  using LT = std::conditional_t<JF, ShLinesP, ShLines>;
+  using LT = std::conditional_t<JF, ShLinesPT<C>, ShLinesT<C>>;
   const LT L = {sh, JF ? ls_padded(N) : N + 1};
   if constexpr (PL::n == 1) {
-    fft_stage_io<PL::r0, S, PPT, SRC_SH && DST_SH, LD, ST, JF>(N, nl, 1, tw, src, dst);
+    fft_stage_io<PL::r0, S, PPT, SRC_SH && DST_SH, LD, ST, JF, C>(N, nl, 1, tw, src, dst);
   } else if constexpr (PL::n == 2) {
-    fft_stage_io<PL::r0, S, PPT, SRC_SH, LD, LT, JF>(N, nl, 1, tw, src, L);
+    fft_stage_io<PL::r0, S, PPT, SRC_SH, LD, LT, JF, C>(N, nl, 1, tw, src, L);
     __syncthreads();
-    fft_stage_io<PL::r1, S, PPT, DST_SH, LT, ST, JF>(N, nl, PL::r0, tw, L, dst);
+    fft_stage_io<PL::r1, S, PPT, DST_SH, LT, ST, JF, C>(N, nl, PL::r0, tw, L, dst);
   } else {
     // staged table (JF): stage 2's block first, then stage 3's
-    const cxd* tw3 = JF ? tw + (PL::r1 - 1) * PL::r0 : tw;
-    fft_stage_io<PL::r0, S, PPT, SRC_SH, LD, LT, JF>(N, nl, 1, tw, src, L);
+    const C* tw3 = JF ? tw + (PL::r1 - 1) * PL::r0 : tw;
+    fft_stage_io<PL::r0, S, PPT, SRC_SH, LD, LT, JF, C>(N, nl, 1, tw, src, L);
     __syncthreads();
-    fft_stage_io<PL::r1, S, PPT, true, LT, LT, JF>(N, nl, PL::r0, tw, L, L);
+    fft_stage_io<PL::r1, S, PPT, true, LT, LT, JF, C>(N, nl, PL::r0, tw, L, L);
     __syncthreads();
-    fft_stage_io<PL::r2, S, PPT, DST_SH, LT, ST, JF>(N, nl, PL::r0 * PL::r1, tw3, L, dst);
+    fft_stage_io<PL::r2, S, PPT, DST_SH, LT, ST, JF, C>(N, nl, PL::r0 * PL::r1, tw3, L, dst);
   }
 }
 
 // NT > 0: the compile-time plan of length NT; NT = 0: the runtime plan of N.
-template <int NT, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF = false, typename LD, typename ST>
-__device__ __forceinline__ void fft_sel(int N, int nl, const cxd* __restrict__ tw, cxd* sh, const LD& src,
+template <int NT, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF = false, typename LD, typename ST, typename C>
+__device__ __forceinline__ void fft_sel(int N, int nl, const C* __restrict__ tw, C* sh, const LD& src,
                                         const ST& dst) {
   if constexpr (NT > 0) {
     fft_fixed<NT, S, PPT, SRC_SH, DST_SH, JF>(nl, tw, sh, src, dst);

@@ -19,6 +19,7 @@ struct Geometry {
   int P, m, MS;        // line-solve group: P lanes, m rows per lane, slab stride
   int Ty;              // y tile of the transforms (divides ny)
   int pptx, pptz;      // FFT points per thread of the x and z transforms (8: the low-register plans)
+  int mp;              // mixed precision: Z, Pp, Q and their transforms in FP32 (complex64)
 };
 
 struct DeviceState {
@@ -33,6 +34,8 @@ struct DeviceState {
   double* gdamp;        // gdamp(-nz:nz, 0:nx)
   double2* twx;         // exp(-2 pi i e / (2 nxd)), then the staged table of the x kernel's 8-point plan
   double2* twz;         // exp(-2 pi i e / nzd)
+  float2* twxf;         // the same tables in FP32 (mixed precision)
+  float2* twzf;
   unsigned long long* cfl;  // running max (bits of a non-negative double)
   int* err;                 // set by a kernel whose bounded wait ran out
   // TMA maps of Z and Pp as 4-D f64 tensors {2 Ty, nxB, nzd ny/Ty, comps}
@@ -73,6 +76,9 @@ cudaError_t make_transform_maps(const Geometry& g, DeviceState& d);
 // the stage-ordered twiddles of the 8-point plan of N into out (at most N
 // entries); returns their number, 0 for a length without such a plan
 int staged_twiddles(int N, double2* out);
+int staged_twiddles(int N, float2* out);
+// a transform length of the mixed-precision form
+bool mp_length_ok(int n);
 // the constant twiddles of the register DFTs, once per device
 cudaError_t set_fft_constants();
 // a transform length the FFT kernels support

@@ -309,7 +309,10 @@ constexpr int RT_WARPS = 4;
 #endif
 constexpr int RT_WAIT_LIMIT = 1 << 22;
 
-template <bool EXACT, bool NONLIN>
+// QT: the complex type of the product spectra Q (float2 in the mixed-
+// precision form: the window lands as FP32 and each value is widened to
+// FP64 where it is read)
+template <bool EXACT, bool NONLIN, typename QT>
 __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs a, int* __restrict__ err) {
   extern __shared__ __align__(128) double2 smt[];
   __shared__ __align__(8) uint64_t bars[RT_WARPS][2];
@@ -330,22 +333,24 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
   const size_t cbase = (size_t)col * g.rows;  // row -2 of the column
   const double2* Vg[3] = {a.V1, a.V2, a.V3};
   // lane 0 queues the copies of tile t into stage t & 1
+  const QT* Qg = reinterpret_cast<const QT*>(a.Q);
+  constexpr unsigned QE = sizeof(QT);
   auto issue = [&](int t) {
     const int stg = t & 1;
     double2* S = st0 + stg * RT_STAGE;
     const int r0 = t * 32;
-    mbar_arrive_expect_tx(&bar[stg], RT_STAGE * 16);
+    mbar_arrive_expect_tx(&bar[stg], (3 * RT_W + 2 * 32) * 16 + 6 * RT_W * QE);
 #pragma unroll
     for (int c = 0; c < 3; ++c) bulk_g2s(S + c * RT_W, Vg[c] + cbase + r0, RT_W * 16, &bar[stg]);
 #pragma unroll 1
     for (int p = 0; p < 6; ++p) {
-      const double2* Qc = a.Q + ((size_t)p * g.ncol + col) * ny;
-      double2* D = S + 3 * RT_W + p * RT_W;
+      const QT* Qc = Qg + ((size_t)p * g.ncol + col) * ny;
+      QT* D = reinterpret_cast<QT*>(S + 3 * RT_W) + p * RT_W;
       const int lo = r0 - 2, hi = r0 + 34;
       const int m0 = lo < 0 ? 0 : lo, m1 = hi > ny ? ny : hi;
-      if (lo < 0) bulk_g2s(D, Qc + ny + lo, (unsigned)(-lo) * 16, &bar[stg]);
-      bulk_g2s(D + (m0 - lo), Qc + m0, (unsigned)(m1 - m0) * 16, &bar[stg]);
-      if (hi > ny) bulk_g2s(D + (ny - lo), Qc, (unsigned)(hi - ny) * 16, &bar[stg]);
+      if (lo < 0) bulk_g2s(D, Qc + ny + lo, (unsigned)(-lo) * QE, &bar[stg]);
+      bulk_g2s(D + (m0 - lo), Qc + m0, (unsigned)(m1 - m0) * QE, &bar[stg]);
+      if (hi > ny) bulk_g2s(D + (ny - lo), Qc, (unsigned)(hi - ny) * QE, &bar[stg]);
     }
     bulk_g2s(S + 9 * RT_W, a.O1 + cbase + 2 + r0, 32 * 16, &bar[stg]);
     bulk_g2s(S + 9 * RT_W + 32, a.O2 + cbase + 2 + r0, 32 * 16, &bar[stg]);
@@ -369,8 +374,10 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
     const double2* S = st0 + stg * RT_STAGE;
     const int r = t * 32 + lane;
     auto tv = [&](int c, int j) -> cxd { return S[c * RT_W + lane + j]; };
+    const QT* SQ = reinterpret_cast<const QT*>(S + 3 * RT_W);
     auto tq = [&](int p, int j) -> cxd {
-      cxd q = S[3 * RT_W + p * RT_W + lane + j];
+      const QT qv = SQ[p * RT_W + lane + j];
+      cxd q = mkc((double)qv.x, (double)qv.y);
       const int row = r + j - 2;
       if (row < 0) return cmul(q, cconj(cc.ph_t));
       if (row >= ny) return cmul(q, cc.ph_t);
@@ -403,11 +410,20 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
   const Geometry& g = a.g;
   if (MODE == COL_RHS && g.ny % 32 == 0 && a.tiled) {  // TMA-staged tiles
     const size_t smem = (size_t)RT_WARPS * 2 * RT_STAGE * sizeof(double2);
-    cudaFuncSetAttribute(k_rhs_tiled<EXACT, NONLIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int blocks = (g.ncol + RT_WARPS - 1) / RT_WARPS;
-    k_rhs_tiled<EXACT, NONLIN><<<blocks, 32 * RT_WARPS, smem, st>>>(a, a.err);
+    if (g.mp) {
+      cudaFuncSetAttribute(k_rhs_tiled<EXACT, NONLIN, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      k_rhs_tiled<EXACT, NONLIN, float2><<<blocks, 32 * RT_WARPS, smem, st>>>(a, a.err);
+    } else {
+      cudaFuncSetAttribute(k_rhs_tiled<EXACT, NONLIN, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      k_rhs_tiled<EXACT, NONLIN, double2><<<blocks, 32 * RT_WARPS, smem, st>>>(a, a.err);
+    }
     return cudaGetLastError();
   }
+  // the untiled and fused forms read FP64 product spectra only
+  if (MODE != COL_SOLVE && g.mp) return cudaErrorInvalidValue;
   if (MODE == COL_RHS) {  // one warp per column, four per block, no shared memory
     const int blocks = (g.ncol + 3) / 4;
     k_column<32, EXACT, NONLIN, COL_RHS><<<blocks, 128, 0, st>>>(a);

@@ -24,11 +24,15 @@ namespace hst {
 
 cudaError_t set_fft_constants() {
   double2 w[48];
+  float2 wf[48];
   for (int k = 0; k < 48; ++k) {
     long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / 48.0L;
     w[k] = make_double2((double)cosl(a), (double)sinl(a));
+    wf[k] = make_float2((float)cosl(a), (float)sinl(a));
   }
-  return cudaMemcpyToSymbol(c_w48, w, sizeof w);
+  cudaError_t e = cudaMemcpyToSymbol(c_w48, w, sizeof w);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_w48f, wf, sizeof wf);
+  return e;
 }
 
 bool fft_length_ok(int n) { return plan_ok(n); }
@@ -37,48 +41,60 @@ bool fft_length_ok(int n) { return plan_ok(n); }
 // assemble_vvdz + IFT (src/hst_transforms.f90:33-54, src/hst_fft.f90:195-207):
 // line yi of the block is row y0 + yi of one x mode of one component; the
 // z modes -nz..nz sit at padded index iz (iz >= 0) or nzd + iz.
+// C: the complex type of the transforms (double2; float2 in the
+// mixed-precision form, where V is read as FP64 and rounded once)
+template <typename C>
+__device__ __forceinline__ C to_c(double2 v) {
+  typedef typename RealOf<C>::T T;
+  return C{(T)v.x, (T)v.y};
+}
+template <typename C>
 struct ZinvSrc {
   const double2* __restrict__ col;  // V + (ix nzT) rows + 2 + y0: row y0 of iz = -nz
   int rows, nz, NZ;
-  __device__ __forceinline__ cxd operator()(int yi, int kz) const {
+  __device__ __forceinline__ C operator()(int yi, int kz) const {
     int iz;
     if (kz <= nz) iz = kz;
     else if (kz >= NZ - nz) iz = kz - NZ;
-    else return mkc(0.0, 0.0);
-    return col[(size_t)(iz + nz) * rows + yi];
+    else return C{0, 0};
+    return to_c<C>(col[(size_t)(iz + nz) * rows + yi]);
   }
 };
+template <typename C>
 struct TileDst {  // one (component, y tile, x mode) z-line set of Z / Pp
-  double2* __restrict__ base;
+  C* __restrict__ base;
   size_t zstride;
-  __device__ __forceinline__ void operator()(int yi, int kz, cxd v) const { base[(size_t)kz * zstride + yi] = v; }
+  __device__ __forceinline__ void operator()(int yi, int kz, C v) const { base[(size_t)kz * zstride + yi] = v; }
 };
+template <typename C>
 struct TileSrc {
-  const double2* __restrict__ base;
+  const C* __restrict__ base;
   size_t zstride;
-  __device__ __forceinline__ cxd operator()(int yi, int kz) const { return base[(size_t)kz * zstride + yi]; }
+  __device__ __forceinline__ C operator()(int yi, int kz) const { return base[(size_t)kz * zstride + yi]; }
 };
 
-template <int NT, int PPT>
+template <int NT, int PPT, typename C>
 __global__ void __launch_bounds__(PPT <= 8 ? 512 : 256) k_zinv(Geometry g, const double2* __restrict__ V0,
                                               const double2* __restrict__ V1, const double2* __restrict__ V2,
-                                              double2* __restrict__ Z, const double2* __restrict__ twz) {
-  extern __shared__ double2 sh[];
+                                              C* __restrict__ Z, const C* __restrict__ twz) {
+  extern __shared__ double2 sh_d[];
+  C* sh = reinterpret_cast<C*>(sh_d);
   const int yt = blockIdx.x, ix = blockIdx.y, c = blockIdx.z;
   const int Ty = g.Ty, NZ = g.nzd, nyT = g.ny / Ty;
   const double2* V = c == 0 ? V0 : (c == 1 ? V1 : V2);
-  const ZinvSrc src = {V + (size_t)ix * g.nzT * g.rows + 2 + yt * Ty, g.rows, g.nz, NZ};
-  const TileDst dst = {Z + (((size_t)c * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
+  const ZinvSrc<C> src = {V + (size_t)ix * g.nzT * g.rows + 2 + yt * Ty, g.rows, g.nz, NZ};
+  const TileDst<C> dst = {Z + (((size_t)c * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
   fft_sel<NT, +1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
 }
 
 // --------------------------------------------------------------- k_zfwd ----
 // transpose_xTOz + FFT (src/hst_transforms.f90:135-139, src/hst_fft.f90:181-193)
 // keeping the 2nz+1 retained modes, stored without ghost rows.
+template <typename C>
 struct ZfwdDst {
-  double2* __restrict__ base;  // Q + (p ncol + ix nzT) ny + y0
+  C* __restrict__ base;  // Q + (p ncol + ix nzT) ny + y0
   int ny, nz, NZ;
-  __device__ __forceinline__ void operator()(int yi, int k, cxd v) const {
+  __device__ __forceinline__ void operator()(int yi, int k, C v) const {
     int iz;
     if (k <= nz) iz = k;
     else if (k >= NZ - nz) iz = k - NZ;
@@ -90,14 +106,15 @@ struct ZfwdDst {
 // (the explicit one-block minimum lets the compiler take 160 registers
 // here, which measured 0.46 against 0.50 ms at 384^2 x 256; the same on
 // k_zinv measured slower)
-template <int NT, int PPT>
-__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256, 1) k_zfwd(Geometry g, const double2* __restrict__ Pp, double2* __restrict__ Q,
-                                              const double2* __restrict__ twz) {
-  extern __shared__ double2 sh[];
+template <int NT, int PPT, typename C>
+__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256, 1) k_zfwd(Geometry g, const C* __restrict__ Pp, C* __restrict__ Q,
+                                              const C* __restrict__ twz) {
+  extern __shared__ double2 sh_d[];
+  C* sh = reinterpret_cast<C*>(sh_d);
   const int yt = blockIdx.x, ix = blockIdx.y, p = blockIdx.z;
   const int Ty = g.Ty, NZ = g.nzd, nyT = g.ny / Ty;
-  const TileSrc src = {Pp + (((size_t)p * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
-  const ZfwdDst dst = {Q + ((size_t)p * g.ncol + (size_t)ix * g.nzT) * g.ny + yt * Ty, g.ny, g.nz, NZ};
+  const TileSrc<C> src = {Pp + (((size_t)p * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
+  const ZfwdDst<C> dst = {Q + ((size_t)p * g.ncol + (size_t)ix * g.nzT) * g.ny + yt * Ty, g.ny, g.nz, NZ};
   fft_sel<NT, -1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
 }
 
@@ -109,15 +126,16 @@ __global__ void __launch_bounds__(PPT <= 8 ? 512 : 256, 1) k_zfwd(Geometry g, co
 // of the pair on the way in; (uu, vv), (ww, uv), (vw, uw) of each row on
 // the way out, separated by Hermitian symmetry.  The c2r reads only the
 // real part of the kx = 0 mode, as FFTW's and cuFFT's c2r do.
+template <typename C>
 struct XinvSrc {
-  const double2* __restrict__ zb;  // Z tile of component 0 at (y tile, kz), + row offset in the tile
-  size_t cs;                       // component stride of Z
+  const C* __restrict__ zb;  // Z tile of component 0 at (y tile, kz), + row offset in the tile
+  size_t cs;                 // component stride of Z
   int Ty, nx, NX;
-  __device__ __forceinline__ cxd operator()(int l, int k) const {
+  __device__ __forceinline__ C operator()(int l, int k) const {
     const int m = k <= nx ? k : (k >= NX - nx ? NX - k : -1);
-    if (m < 0) return mkc(0.0, 0.0);
-    const double2* p = zb + (size_t)m * Ty;
-    cxd a, b;
+    if (m < 0) return C{0, 0};
+    const C* p = zb + (size_t)m * Ty;
+    C a, b;
     if (l == 0) {  // u(y0) + i v(y0)
       a = p[0];
       b = p[cs];
@@ -128,20 +146,21 @@ struct XinvSrc {
       a = p[2 * cs];
       b = p[2 * cs + 1];
     }
-    if (k == 0) return mkc(a.x, b.x);
-    if (k <= nx) return mkc(a.x - b.y, a.y + b.x);
-    return mkc(a.x + b.y, b.x - a.y);  // conj(a) + i conj(b)
+    if (k == 0) return C{a.x, b.x};
+    if (k <= nx) return C{a.x - b.y, a.y + b.x};
+    return C{a.x + b.y, b.x - a.y};  // conj(a) + i conj(b)
   }
 };
 // The same from the block's staging copy of the tile, [comp 3][nxB][row 2]
 // (landed by TMA)
+template <typename C>
 struct XinvSh {
-  const double2* s;
+  const C* s;
   int nxB, nx, NX;
-  __device__ __forceinline__ cxd operator()(int l, int k) const {
+  __device__ __forceinline__ C operator()(int l, int k) const {
     const int m = k <= nx ? k : (k >= NX - nx ? NX - k : -1);
-    if (m < 0) return mkc(0.0, 0.0);
-    cxd a, b;
+    if (m < 0) return C{0, 0};
+    C a, b;
     if (l == 0) {
       a = s[2 * m];
       b = s[2 * (nxB + m)];
@@ -152,23 +171,24 @@ struct XinvSh {
       a = s[2 * (2 * nxB + m)];
       b = s[2 * (2 * nxB + m) + 1];
     }
-    if (k == 0) return mkc(a.x, b.x);
-    if (k <= nx) return mkc(a.x - b.y, a.y + b.x);
-    return mkc(a.x + b.y, b.x - a.y);
+    if (k == 0) return C{a.x, b.x};
+    if (k <= nx) return C{a.x - b.y, a.y + b.x};
+    return C{a.x + b.y, b.x - a.y};
   }
 };
 // the products of row yy, pair pl (0: uu, vv; 1: ww, uv; 2: vw, uw) at x
-template <typename LT>
+template <typename LT, typename C>
 struct ProdSrc {
+  typedef typename RealOf<C>::T T;
   LT L;
-  double f;
-  __device__ __forceinline__ cxd operator()(int l, int x) const {
+  T f;
+  __device__ __forceinline__ C operator()(int l, int x) const {
     const int yy = l >= 3 ? 1 : 0, pl = l - 3 * yy;
-    const cxd a = L(yy, x), b = L(2, x);
-    const double u = a.x, v = a.y, w = yy ? b.y : b.x;
-    if (pl == 0) return mkc(u * u * f, v * v * f);
-    if (pl == 1) return mkc(w * w * f, u * v * f);
-    return mkc(v * w * f, u * w * f);
+    const C a = L(yy, x), b = L(2, x);
+    const T u = a.x, v = a.y, w = yy ? b.y : b.x;
+    if (pl == 0) return C{u * u * f, v * v * f};
+    if (pl == 1) return C{w * w * f, u * v * f};
+    return C{v * w * f, u * w * f};
   }
 };
 
@@ -188,20 +208,22 @@ constexpr int XPROD_WAIT_LIMIT = 1 << 22;  // polls of the tile's TMA barrier be
 // addresses, and the dynamic shared base is only known to be 16-byte
 // aligned), then the mbarrier and the tile flag
 __host__ __device__ inline int xprod_stage_off(int NX) { return 6 * ls_padded(NX); }
-__host__ __device__ inline size_t xprod_tma_smem(int NX, int nxB) {
-  return ((size_t)xprod_stage_off(NX) + 12 * (size_t)nxB + 2) * sizeof(double2) + 128;
+__host__ __device__ inline size_t xprod_tma_smem(int NX, int nxB, size_t elem) {
+  return ((size_t)xprod_stage_off(NX) + 12 * (size_t)nxB + 2) * elem + 128;
 }
 
-template <int NT, int PPT>
+template <int NT, int PPT, typename C>
 __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, PPT))
-    k_xprod(Geometry g, const double2* __restrict__ Z, double2* __restrict__ Pp, const double2* __restrict__ twx,
+    k_xprod(Geometry g, const C* __restrict__ Z, C* __restrict__ Pp, const C* __restrict__ twx,
             const double* __restrict__ dyl, PhysScalars ps, int want_cfl, unsigned long long* __restrict__ cflmax,
             const __grid_constant__ CUtensorMap tmZ, const __grid_constant__ CUtensorMap tmP, int* __restrict__ err) {
-  extern __shared__ double2 sh[];
+  typedef typename RealOf<C>::T T;
+  extern __shared__ double2 sh_d[];
+  C* sh = reinterpret_cast<C*>(sh_d);
   // 8-point plans: butterflies index-fastest over padded shared lines, the
   // tile in and out by TMA
   constexpr bool JF = (PPT <= 8 && NT > 0);
-  using LT = std::conditional_t<JF, ShLinesP, ShLines>;
+  using LT = std::conditional_t<JF, ShLinesPT<C>, ShLinesT<C>>;
   const int NX = 2 * g.nxd, nx = g.nx, nxB = g.nxB, NZ = g.nzd, Ty = g.Ty, LS = JF ? ls_padded(NX) : NX + 1;
   const int nyT = g.ny / Ty;
   const int y0 = 2 * blockIdx.x, kz = blockIdx.y;
@@ -209,8 +231,8 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   const size_t cs = (size_t)NZ * nyT * nxB * Ty;
   const size_t tile = ((size_t)yt * NZ + kz) * nxB * Ty;
   const LT L = {sh, LS};
-  double2* stg = sh + xprod_stage_off(NX);
-  if constexpr (JF) stg += ((128u - (smem_u32(stg) & 127u)) & 127u) / sizeof(double2);
+  C* stg = sh + xprod_stage_off(NX);
+  if constexpr (JF) stg += ((128u - (smem_u32(stg) & 127u)) & 127u) / sizeof(C);
   // u + i v of both rows and w0 + i w1 on the physical x grid
   if constexpr (JF) {
     uint64_t* bar = reinterpret_cast<uint64_t*>(stg + 12 * nxB);
@@ -222,7 +244,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
     if (threadIdx.x == 0) {
       mbar_init(bar, 1);
       fence_mbar_init();
-      mbar_arrive_expect_tx(bar, 3u * nxB * 32u);
+      mbar_arrive_expect_tx(bar, 3u * nxB * 2u * (unsigned)sizeof(C));
       tma_load_4d(stg, &tmZ, 2 * yi0, 0, yt * NZ + kz, 0, bar);
       bool ok = mbar_wait_bounded(bar, 0, XPROD_WAIT_LIMIT);
       if (!ok) {
@@ -235,10 +257,10 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
     }
     __syncthreads();
     if (!tile_ok) return;
-    const XinvSh xs = {stg, nxB, nx, NX};
+    const XinvSh<C> xs = {stg, nxB, nx, NX};
     fft_sel<NT, +1, PPT, false, true, JF>(NX, 3, twx + NX, sh, xs, L);
   } else {
-    const XinvSrc xs = {Z + tile + yi0, cs, Ty, nx, NX};
+    const XinvSrc<C> xs = {Z + tile + yi0, cs, Ty, nx, NX};
     fft_sel<NT, +1, PPT, false, true, JF>(NX, 3, twx, sh, xs, L);
   }
   __syncthreads();
@@ -246,16 +268,16 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
     double cm = 0.0;
     const double rdy0 = dyl[y0], rdy1 = dyl[y0 + 1];
     for (int x = threadIdx.x; x < NX; x += blockDim.x) {
-      cxd a0 = L(0, x), a1 = L(1, x), b = L(2, x);
-      double c0 = fabs(a0.x) / ps.dx + fabs(a0.y) / rdy0 + fabs(b.x) / ps.dz;
-      double c1 = fabs(a1.x) / ps.dx + fabs(a1.y) / rdy1 + fabs(b.y) / ps.dz;
+      const C a0 = L(0, x), a1 = L(1, x), b = L(2, x);
+      double c0 = fabs((double)a0.x) / ps.dx + fabs((double)a0.y) / rdy0 + fabs((double)b.x) / ps.dz;
+      double c1 = fabs((double)a1.x) / ps.dx + fabs((double)a1.y) / rdy1 + fabs((double)b.y) / ps.dz;
       cm = fmax(cm, fmax(c0, c1));
     }
     for (int o = 16; o > 0; o >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
     if ((threadIdx.x & 31) == 0) atomicMax(cflmax, (unsigned long long)__double_as_longlong(cm));
   }
   // the six product lines, transformed forward in place
-  const ProdSrc<LT> ps6 = {L, ps.factor};
+  const ProdSrc<LT, C> ps6 = {L, (T)ps.factor};
   fft_sel<NT, -1, PPT, true, true, JF>(NX, 6, JF ? twx + NX : twx, sh, ps6, L);
   __syncthreads();
   // separate the two real transforms of each line, keep kx = 0..nx
@@ -264,9 +286,10 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
 #pragma unroll
     for (int yy = 0; yy < 2; ++yy) {
       const int ln = pl + 3 * yy;
-      cxd Zk = L(ln, ix), Zm = L(ln, ix == 0 ? 0 : NX - ix);
-      cxd X = mkc(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y));
-      cxd Y = mkc(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x));
+      const C Zk = L(ln, ix), Zm = L(ln, ix == 0 ? 0 : NX - ix);
+      const T h = T(0.5);
+      const C X = C{h * (Zk.x + Zm.x), h * (Zk.y - Zm.y)};
+      const C Y = C{h * (Zk.y + Zm.y), h * (Zm.x - Zk.x)};
       if constexpr (JF) {
         stg[((2 * pl) * nxB + ix) * 2 + yy] = X;
         stg[((2 * pl + 1) * nxB + ix) * 2 + yy] = Y;
@@ -292,8 +315,8 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
 // ------------------------------------------------------- staged twiddles ----
 // The twiddles of the 8-point plan of N in stage order (see fft_stage_io):
 // for each stage after the first, [r - 1][kk] = W_N^(kk r N/(Ns R)).
-template <int N>
-static int staged_twiddles_t(double2* out) {
+template <int N, typename C>
+static int staged_twiddles_t(C* out) {
   using PL = Plan8<N>;
   const int rad[3] = {PL::r0, PL::r1, PL::r2};
   int n = 0, Ns = 1;
@@ -304,7 +327,8 @@ static int staged_twiddles_t(double2* out) {
         for (int kk = 0; kk < Ns; ++kk) {
           const long e = (long)kk * r * (N / (Ns * R)) % N;
           long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)e / (long double)N;
-          out[n++] = make_double2((double)cosl(a), (double)sinl(a));
+          out[n].x = (typename RealOf<C>::T)cosl(a);
+          out[n++].y = (typename RealOf<C>::T)sinl(a);
         }
     Ns *= R;
   }
@@ -319,6 +343,14 @@ int staged_twiddles(int N, double2* out) {
   }
   return 0;
 }
+int staged_twiddles(int N, float2* out) {
+  switch (N) {
+    case 192: return staged_twiddles_t<192>(out);
+    case 384: return staged_twiddles_t<384>(out);
+    case 768: return staged_twiddles_t<768>(out);
+  }
+  return 0;
+}
 
 // ------------------------------------------------------------- TMA maps ----
 // Z and Pp seen as 4-D f64 tensors: d0 = the 2 Ty doubles of one y tile
@@ -326,7 +358,7 @@ int staged_twiddles(int N, double2* out) {
 // The x kernel's box is {4 doubles (two rows), nxB, 1, comps}.
 static bool xprod_uses_maps(const Geometry& g) {
   const int NX = 2 * g.nxd;
-  return g.pptx == 8 && (NX == 192 || NX == 384 || NX == 768) && g.nxB <= 256;
+  return (g.pptx == 8 || g.mp) && (NX == 192 || NX == 384 || NX == 768) && g.nxB <= 256;
 }
 
 typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -345,11 +377,11 @@ cudaError_t make_transform_maps(const Geometry& g, DeviceState& d) {
   for (int which = 0; which < 2; ++which) {
     const cuuint32_t comps = which == 0 ? 3 : 6;
     cuuint64_t dims[4] = {(cuuint64_t)2 * g.Ty, (cuuint64_t)g.nxB, (cuuint64_t)g.nzd * nyT, comps};
-    cuuint64_t strides[3] = {(cuuint64_t)16 * g.Ty, (cuuint64_t)16 * g.Ty * g.nxB,
-                             (cuuint64_t)16 * g.Ty * g.nxB * g.nzd * nyT};
+    const cuuint64_t es = g.mp ? 8 : 16;  // bytes of one complex element
+    cuuint64_t strides[3] = {es * g.Ty, es * g.Ty * g.nxB, es * g.Ty * g.nxB * g.nzd * nyT};
     cuuint32_t box[4] = {4, (cuuint32_t)g.nxB, 1, comps};
     cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = enc(which == 0 ? &d.tmZ : &d.tmPp, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+    CUresult r = enc(which == 0 ? &d.tmZ : &d.tmPp, g.mp ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
                      which == 0 ? (void*)d.Z : (void*)d.Pp, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
@@ -393,14 +425,44 @@ static void big_smem(K k) {
     }                                                       \
   } while (0)
 
+// The mixed-precision form compiles the transforms for the lengths its
+// workloads use: 8 points a thread at 192, 384 and 768, 16 at 96.
+#define HST_FFT_DISPATCH_MP(N, CALL)   \
+  do {                                 \
+    switch (N) {                       \
+      case 96: CALL(96, 16) break;     \
+      case 192: CALL(192, 8) break;    \
+      case 384: CALL(384, 8) break;    \
+      case 768: CALL(768, 8) break;    \
+      default:                         \
+        return cudaErrorInvalidValue;  \
+    }                                  \
+  } while (0)
+
+bool mp_length_ok(int n) { return n == 96 || n == 192 || n == 384 || n == 768; }
+
 cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st) {
   const int pts = g.nzd * g.Ty;
-  const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(double2);
   const dim3 grid(g.ny / g.Ty, g.nxB, 3);
-#define HST_ZINV(NT, PPT)                                                                               \
-  {                                                                                                     \
-    big_smem(k_zinv<NT, PPT>);                                                                          \
-    k_zinv<NT, PPT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], d.Z, d.twz); \
+  if (g.mp) {
+    typedef float2 C;
+    const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
+    C* Z = reinterpret_cast<C*>(d.Z);
+#define HST_ZINV(NT, PPT)                                                                                     \
+  {                                                                                                           \
+    big_smem(k_zinv<NT, PPT, C>);                                                                             \
+    k_zinv<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], Z, d.twzf);      \
+  }
+    HST_FFT_DISPATCH_MP(g.nzd, HST_ZINV);
+#undef HST_ZINV
+    return cudaGetLastError();
+  }
+  typedef double2 C;
+  const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
+#define HST_ZINV(NT, PPT)                                                                                     \
+  {                                                                                                           \
+    big_smem(k_zinv<NT, PPT, C>);                                                                             \
+    k_zinv<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], d.Z, d.twz);     \
   }
   HST_FFT_DISPATCH(g.nzd, pts, g.pptz == 8, HST_ZINV);
 #undef HST_ZINV
@@ -409,12 +471,27 @@ cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st
 
 cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st) {
   const int pts = g.nzd * g.Ty;
-  const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(double2);
   const dim3 grid(g.ny / g.Ty, g.nxB, 6);
-#define HST_ZFWD(NT, PPT)                                                            \
-  {                                                                                  \
-    big_smem(k_zfwd<NT, PPT>);                                                       \
-    k_zfwd<NT, PPT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Pp, d.Q, d.twz); \
+  if (g.mp) {
+    typedef float2 C;
+    const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
+    const C* Pp = reinterpret_cast<const C*>(d.Pp);
+    C* Q = reinterpret_cast<C*>(d.Q);
+#define HST_ZFWD(NT, PPT)                                                                  \
+  {                                                                                        \
+    big_smem(k_zfwd<NT, PPT, C>);                                                          \
+    k_zfwd<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, Pp, Q, d.twzf);       \
+  }
+    HST_FFT_DISPATCH_MP(g.nzd, HST_ZFWD);
+#undef HST_ZFWD
+    return cudaGetLastError();
+  }
+  typedef double2 C;
+  const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
+#define HST_ZFWD(NT, PPT)                                                                  \
+  {                                                                                        \
+    big_smem(k_zfwd<NT, PPT, C>);                                                          \
+    k_zfwd<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Pp, d.Q, d.twz);    \
   }
   HST_FFT_DISPATCH(g.nzd, pts, g.pptz == 8, HST_ZFWD);
 #undef HST_ZFWD
@@ -425,14 +502,31 @@ cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScal
                          cudaStream_t st) {
   const int NX = 2 * g.nxd;
   const int pts = 6 * NX;
-  const size_t smem = xprod_uses_maps(g) ? xprod_tma_smem(NX, g.nxB) : (size_t)6 * (NX + 1) * sizeof(double2);
   if (xprod_uses_maps(g) != d.maps) return cudaErrorInvalidValue;
   const dim3 grid(g.ny / 2, g.nzd);
-#define HST_XPROD(NT, PPT)                                                                                   \
-  {                                                                                                          \
-    big_smem(k_xprod<NT, PPT>);                                                                              \
-    k_xprod<NT, PPT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Z, d.Pp, d.twx, d.dyl, ph, want_cfl,    \
-                                                                 d.cfl, d.tmZ, d.tmPp, d.err);               \
+  if (g.mp) {
+    typedef float2 C;
+    const size_t smem =
+        xprod_uses_maps(g) ? xprod_tma_smem(NX, g.nxB, sizeof(C)) : (size_t)6 * (NX + 1) * sizeof(C);
+    const C* Z = reinterpret_cast<const C*>(d.Z);
+    C* Pp = reinterpret_cast<C*>(d.Pp);
+#define HST_XPROD(NT, PPT)                                                                                    \
+  {                                                                                                           \
+    big_smem(k_xprod<NT, PPT, C>);                                                                            \
+    k_xprod<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, Z, Pp, d.twxf, d.dyl, ph, want_cfl,     \
+                                                                    d.cfl, d.tmZ, d.tmPp, d.err);             \
+  }
+    HST_FFT_DISPATCH_MP(NX, HST_XPROD);
+#undef HST_XPROD
+    return cudaGetLastError();
+  }
+  typedef double2 C;
+  const size_t smem = xprod_uses_maps(g) ? xprod_tma_smem(NX, g.nxB, sizeof(C)) : (size_t)6 * (NX + 1) * sizeof(C);
+#define HST_XPROD(NT, PPT)                                                                                    \
+  {                                                                                                           \
+    big_smem(k_xprod<NT, PPT, C>);                                                                            \
+    k_xprod<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Z, d.Pp, d.twx, d.dyl, ph, want_cfl,  \
+                                                                    d.cfl, d.tmZ, d.tmPp, d.err);             \
   }
   HST_FFT_DISPATCH(NX, pts, g.pptx == 8, HST_XPROD);
 #undef HST_XPROD

@@ -47,6 +47,7 @@ class Params(ct.Structure):
         ("damp_edge", ct.c_double), ("damp_norm", ct.c_double), ("damp_angle", ct.c_double),
         ("damp_hard", ct.c_int), ("damp_mean", ct.c_int), ("damp_follow", ct.c_int),
         ("device", ct.c_int),
+        ("precision", ct.c_int),
     ]
 
 
@@ -111,6 +112,7 @@ DECK_DEFAULTS = dict(  # src/hst_input.f90:140-155
     # that a deck using it is refused, not run without it
     sl_amplitude=0.0, sl_period=0.0, sl_delta=0.0, sl_start=0.0, sl_bodyforce=False, sl_ramp=False,
 )
+PREC_FP64, PREC_MIXED = 0, 1  # hst_gpu_params.precision
 
 
 def read_deck(path) -> dict:
@@ -198,6 +200,8 @@ class Solver:
         p.damp_hard, p.damp_mean, p.damp_follow = int(bool(cfg["damp_hard"])), int(bool(cfg["damp_mean"])), int(
             bool(cfg["damp_follow"]))
         p.device = int(device)
+        prec = cfg.get("precision", PREC_FP64)
+        p.precision = {"fp64": PREC_FP64, "mixed": PREC_MIXED}.get(prec, prec) if isinstance(prec, str) else int(prec)
         self.params = p
         self._h = ct.c_void_p()
         rc = lib().hst_gpu_create(ct.byref(p), ct.byref(self._h))

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define HST_GPU_ABI_VERSION 1
+#define HST_GPU_ABI_VERSION 2
 
 /* status classes */
 #define HST_OK 0
@@ -55,6 +55,13 @@ extern "C" {
 #define HST_OLD2 4
 #define HST_RHS1 5
 #define HST_RHS2 6
+
+/* precision of the context (hst_gpu_params.precision) */
+#define HST_PREC_FP64 0  /* everything in FP64: the drop-in */
+#define HST_PREC_MIXED 1 /* the x-z transforms, the products and their spectra in FP32; the right-hand
+                            sides, the shear shift, the line solves and u, w in FP64.  Needs 2 nxd and
+                            nzd in {96, 192, 384, 768} and ny a multiple of 32.  No counterpart in the
+                            reference, which is FP64 throughout. */
 
 /* line-solve kinds, KIND_D2V .. KIND_DY (src/hst_linsolve.f90:83) */
 #define HST_KIND_D2V 1
@@ -75,7 +82,8 @@ typedef struct hst_gpu_params {
   double s2_mean, s2_amplitude, s2_period, s2_start;
   double damp_kpar, damp_kperp, damp_rate, damp_edge, damp_norm, damp_angle;
   int damp_hard, damp_mean, damp_follow;
-  int device; /* CUDA device ordinal */
+  int device;    /* CUDA device ordinal */
+  int precision; /* HST_PREC_FP64 or HST_PREC_MIXED */
 } hst_gpu_params;
 
 typedef struct hst_ctx hst_ctx;

@@ -357,3 +357,41 @@ def test_async_io_matches_synchronous():
     assert np.array_equal(Va, Vb)
     a.close()
     b.close()
+
+
+# ------------------------------------------------ the mixed-precision form ----
+@pytest.mark.parametrize("deck_over", [dict(), dict(exact_shift=True), dict(nx=63, nz=64, ny=32),
+                                       dict(nx=63, nz=64, ny=32, exact_shift=True, s2_amplitude=0.5,
+                                            s2_period=10.0)])
+def test_mixed_precision_parity(deck_over):
+    """HST_PREC_MIXED (FP32 transforms, products and spectra; FP64 right-hand
+    sides, shift and solves) against the FP64 oracle: relative L2 over the
+    interior rows <= 1e-5 after 30 substeps, the bound the mixed-precision
+    form is held to; and measurably different from the FP64 path (the FP32
+    kernels ran)."""
+    deck = c1_deck(**deck_over)
+    V0 = seeded_field(deck, seed=2, k0=4.0, energy=0.1)
+    s, o = make_pair(dict(deck, precision="mixed"), V0)
+    Vg, Vo = run_pair(s, o, deck["deltat"], 10)
+    err = rel_l2(Vg, Vo)
+    assert err <= 1e-5, (deck_over, err)
+    assert err > 1e-12, err
+    s.close()
+
+
+def test_mixed_precision_against_fp64_at_384():
+    """The 384^2 x 256 workload: 30 substeps of the mixed-precision form
+    against the FP64 form on the same GPU (whose agreement with the oracle
+    the smaller decks pin), relative L2 <= 1e-5."""
+    deck = dict(nx=127, ny=256, nz=128, alfa0=1.0, beta0=1.0, ly=2 * PI, re=2000.0, S=1.0, deltat=0.002)
+    V0 = seeded_field(deck, seed=1, k0=8.0, energy=0.1)
+    a = hst.Solver(deck)
+    b = hst.Solver(dict(deck, precision="mixed"))
+    for s in (a, b):
+        s.set_velocity(V0)
+        for _ in range(10):
+            s.timestep(deck["deltat"])
+    err = rel_l2(b.velocity(), a.velocity())
+    assert err <= 1e-5, err
+    a.close()
+    b.close()
