@@ -361,6 +361,8 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
   }
   const ColConst cc = col_const(col, g, a.ps, a.sc, a.gdamp);
   const SubstepScalars& sc = a.sc;
+  typedef typename RealOf<QT>::T QR;
+  const QT ph_q = QT{(QR)cc.ph_t.x, (QR)cc.ph_t.y};  // the ghost-row phase in the spectra's precision
   for (int t = 0; t < ntile; ++t) {
     const int stg = t & 1;
     if (!mbar_wait_bounded(&bar[stg], (t >> 1) & 1, RT_WAIT_LIMIT)) {
@@ -375,12 +377,11 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
     const int r = t * 32 + lane;
     auto tv = [&](int c, int j) -> cxd { return S[c * RT_W + lane + j]; };
     const QT* SQ = reinterpret_cast<const QT*>(S + 3 * RT_W);
-    auto tq = [&](int p, int j) -> cxd {
-      const QT qv = SQ[p * RT_W + lane + j];
-      cxd q = mkc((double)qv.x, (double)qv.y);
+    auto tq = [&](int p, int j) -> QT {
+      const QT q = SQ[p * RT_W + lane + j];
       const int row = r + j - 2;
-      if (row < 0) return cmul(q, cconj(cc.ph_t));
-      if (row >= ny) return cmul(q, cc.ph_t);
+      if (row < 0) return cmul(q, cconj(ph_q));
+      if (row >= ny) return cmul(q, ph_q);
       return q;
     };
     cxd r1, r2, o1, o2;

@@ -95,14 +95,20 @@ __device__ __forceinline__ void rhs_point(const ColConst& c, const SubstepScalar
   if (NONLIN) {
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
-      cxd q0 = mkc(0, 0), q1 = mkc(0, 0), q2 = mkc(0, 0);
+      // the stencils of the product spectra in their own precision (FP32
+      // in the mixed-precision form), the rest in FP64
+      typedef decltype(tq(0, 0)) QV;
+      typedef typename RealOf<QV>::T QR;
+      QV a0 = QV{0, 0}, a1 = QV{0, 0}, a2 = QV{0, 0};
 #pragma unroll
       for (int j = 0; j < 5; ++j) {
-        cxd qv = tq(p, j);
-        q0 = mkc(q0.x + d0[j] * qv.x, q0.y + d0[j] * qv.y);
-        q1 = mkc(q1.x + d1[j] * qv.x, q1.y + d1[j] * qv.y);
-        q2 = mkc(q2.x + d2[j] * qv.x, q2.y + d2[j] * qv.y);
+        const QV qv = tq(p, j);
+        const QR e0 = (QR)d0[j], e1 = (QR)d1[j], e2 = (QR)d2[j];
+        a0 = QV{a0.x + e0 * qv.x, a0.y + e0 * qv.y};
+        a1 = QV{a1.x + e1 * qv.x, a1.y + e1 * qv.y};
+        a2 = QV{a2.x + e2 * qv.x, a2.y + e2 * qv.y};
       }
+      const cxd q0 = mkc(a0.x, a0.y), q1 = mkc(a1.x, a1.y), q2 = mkc(a2.x, a2.y);
       cxd ru = mkc(0, 0), rw = mkc(0, 0), ex;
       if (p == 0) {  // uu
         ru = mkc(al * q0.y, -al * q0.x);

@@ -198,7 +198,12 @@ struct ProdSrc {
 // launch bounds of k_xprod: 6 NX / PPT threads; the 8-point plan at 384
 // is held to 72 registers so that three 288-thread blocks fit an SM
 constexpr int xprod_threads(int NT, int PPT) { return PPT <= 8 ? (NT == 384 ? 288 : 640) : 320; }
-constexpr int xprod_min_blocks(int NT, int PPT) { return PPT <= 8 && NT == 384 ? XPROD_MINB : 1; }
+#ifndef XPROD_MINB_F32
+#define XPROD_MINB_F32 4
+#endif
+constexpr int xprod_min_blocks(int NT, int PPT, int es) {
+  return PPT <= 8 && NT == 384 ? (es == 8 ? XPROD_MINB_F32 : XPROD_MINB) : 1;
+}
 
 constexpr int XPROD_WAIT_LIMIT = 1 << 22;  // polls of the tile's TMA barrier before giving up
 
@@ -213,7 +218,7 @@ __host__ __device__ inline size_t xprod_tma_smem(int NX, int nxB, size_t elem) {
 }
 
 template <int NT, int PPT, typename C>
-__global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, PPT))
+__global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, PPT, (int)sizeof(C)))
     k_xprod(Geometry g, const C* __restrict__ Z, C* __restrict__ Pp, const C* __restrict__ twx,
             const double* __restrict__ dyl, PhysScalars ps, int want_cfl, unsigned long long* __restrict__ cflmax,
             const __grid_constant__ CUtensorMap tmZ, const __grid_constant__ CUtensorMap tmP, int* __restrict__ err) {
@@ -427,16 +432,18 @@ static void big_smem(K k) {
 
 // The mixed-precision form compiles the transforms for the lengths its
 // workloads use: 8 points a thread at 192, 384 and 768, 16 at 96.
-#define HST_FFT_DISPATCH_MP(N, CALL)   \
-  do {                                 \
-    switch (N) {                       \
-      case 96: CALL(96, 16) break;     \
-      case 192: CALL(192, 8) break;    \
-      case 384: CALL(384, 8) break;    \
-      case 768: CALL(768, 8) break;    \
-      default:                         \
-        return cudaErrorInvalidValue;  \
-    }                                  \
+#define HST_FFT_DISPATCH_MP(N, P16, CALL)          \
+  do {                                             \
+    switch (N) {                                   \
+      case 96: CALL(96, 16) break;                 \
+      case 192:                                    \
+        if (P16) CALL(192, 16) else CALL(192, 8) break; \
+      case 384:                                    \
+        if (P16) CALL(384, 16) else CALL(384, 8) break; \
+      case 768: CALL(768, 8) break;                \
+      default:                                     \
+        return cudaErrorInvalidValue;              \
+    }                                              \
   } while (0)
 
 bool mp_length_ok(int n) { return n == 96 || n == 192 || n == 384 || n == 768; }
@@ -453,7 +460,7 @@ cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st
     big_smem(k_zinv<NT, PPT, C>);                                                                             \
     k_zinv<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], Z, d.twzf);      \
   }
-    HST_FFT_DISPATCH_MP(g.nzd, HST_ZINV);
+    HST_FFT_DISPATCH_MP(g.nzd, g.pptz == 16, HST_ZINV);
 #undef HST_ZINV
     return cudaGetLastError();
   }
@@ -482,7 +489,7 @@ cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st
     big_smem(k_zfwd<NT, PPT, C>);                                                          \
     k_zfwd<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, Pp, Q, d.twzf);       \
   }
-    HST_FFT_DISPATCH_MP(g.nzd, HST_ZFWD);
+    HST_FFT_DISPATCH_MP(g.nzd, g.pptz == 16, HST_ZFWD);
 #undef HST_ZFWD
     return cudaGetLastError();
   }
@@ -516,7 +523,7 @@ cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScal
     k_xprod<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, Z, Pp, d.twxf, d.dyl, ph, want_cfl,     \
                                                                     d.cfl, d.tmZ, d.tmPp, d.err);             \
   }
-    HST_FFT_DISPATCH_MP(NX, HST_XPROD);
+    HST_FFT_DISPATCH_MP(NX, false, HST_XPROD);
 #undef HST_XPROD
     return cudaGetLastError();
   }
