@@ -147,6 +147,82 @@ def seeded_field(cfg, y):
                             energy=0.1)
 
 
+# The ensemble of independent realisations with uneven sizes: 24 members of
+# 192^2 x 128 (deck nx = 63, nz = 64, ny = 128) and 8 of 384^2 x 192 (nx = 95,
+# nz = 96, ny = 192; the reference pads nxd, nzd to 192, 384), seeds 1..32,
+# Re 1500, dt 0.004, k0 6, energy 0.1.
+ENSEMBLE = [dict(nx=63, ny=128, nz=64)] * 24 + [dict(nx=95, ny=192, nz=96)] * 8
+ENSEMBLE_COMMON = dict(alfa0=1.0, beta0=1.0, ly=2 * PI, re=1500.0, S=1.0, deltat=0.004)
+
+
+def run_ensemble(args, dev):
+    """Every member in its own context and stream: the concurrent form queues
+    one time step of each member in turn (hst_gpu_timesteps, no host wait)
+    and times the whole ensemble between two events that all member streams
+    are joined to; the sequential form advances the members one after
+    another with the CFL read-back of every step, as 32 separate plain runs
+    would.  Returns (concurrent, sequential) member-substeps/s and the
+    per-member device bytes."""
+    import torch
+    from homogenenousshearturbulence_b200 import hst
+    members = []
+    for i, sz in enumerate(ENSEMBLE):
+        deck = dict(ENSEMBLE_COMMON, **sz, precision=args.precision)
+        s = hst.Solver(deck, device=dev)
+        V0 = hst.random_field(deck["nx"], deck["ny"], deck["nz"], deck["alfa0"], deck["beta0"], deck["ly"], s.y,
+                              seed=i + 1, k0=6.0, energy=0.1)
+        s.time = 0.0
+        s.set_velocity(V0)
+        members.append(s)
+    dt = ENSEMBLE_COMMON["deltat"]
+    streams = [torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", dev)) for s in members]
+    main = torch.cuda.current_stream(dev)
+
+    def concurrent(k):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        for st in streams:
+            st.wait_event(e0)
+        for _ in range(k):
+            for s in members:
+                s.timesteps(1, dt)
+        for st in streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+        e1.record(main)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def sequential(k):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        for s, st in zip(members, streams):
+            st.wait_event(e0)
+            for _ in range(k):
+                s.timestep(dt)
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+        e1.record(main)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    concurrent(max(3, args.warmup))
+    torch.cuda.synchronize(dev)
+    ms_c = concurrent(args.steps)
+    ms_s = sequential(max(3, args.steps // 3))
+    n = len(members)
+    rate_c = 3 * n * args.steps / (ms_c / 1000.0)
+    rate_s = 3 * n * max(3, args.steps // 3) / (ms_s / 1000.0)
+    cfl_ok = all(math.isfinite(s.compute_cfl()) for s in members)
+    for s in members:
+        s.close()
+    return rate_c, rate_s, ms_c, cfl_ok
+
+
 def reduce_max(x, dist, device=None):
     """The maximum over ranks of a float (the device time of the timed
     region); x itself without a process group."""
@@ -193,17 +269,79 @@ def cpu_oracle_rate(cfg, steps, budget_s=60.0, warmup=1):
     return 3 * n / el, n, threads, 1 + w
 
 
+def ensemble_main(args):
+    """--config c4: the batched ensemble on one GPU (rank 0 of each process
+    runs its own ensemble; the reference arm times the oracle on the first
+    small member, the reference having no batched form)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    unit = "substeps/s"
+    label = ("ensemble of 32 independent realisations in one GPU: 24 x 192^2 x 128 (nx=63, nz=64, ny=128) + "
+             "8 x 384^2 x 192 (nx=95, nz=96, ny=192), Re 1500, dt 0.004, seeds 1..32")
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        cfg = dict(deck=dict(ENSEMBLE_COMMON, **ENSEMBLE[0]), k0=6.0)
+        rate, n, threads, w = cpu_oracle_rate(cfg, args.steps, budget_s=60.0, warmup=args.warmup)
+        # the members one after another: a substep of every member takes
+        # 24 small and 8 large member-substeps
+        small = rate
+        big_cfg = dict(deck=dict(ENSEMBLE_COMMON, **ENSEMBLE[-1]), k0=6.0)
+        rate_b, nb, _, _ = cpu_oracle_rate(big_cfg, 1, budget_s=30.0, warmup=1)
+        per_step = 24 / small + 8 / rate_b  # seconds per substep of every member
+        agg = 32 / per_step
+        line = {"metric": "substeps_per_s", "value": agg, "unit": unit, "impl": "reference", "n_gpus": args.gpus,
+                "steps": n, "warmup": w, "ms_per_step": 3000.0 * 32 / agg, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": label, "members": 32},
+                "cpu_baseline": {"value": agg, "unit": unit, "cores": threads, "kind": "port",
+                                 "sample": f"{n} + {nb} time steps of a small and a large member (oracle, all host "
+                                           f"threads), the members taken one after another"},
+                "e2e": {"value": agg, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    rate_c, rate_s, ms_c, ok = run_ensemble(args, local)
+    ms = reduce_max(ms_c, dist, f"cuda:{local}")
+    value = whole_job_rate(world, 3 * 32 * args.steps, ms)
+    if rank == 0:
+        line = {"metric": "substeps_per_s", "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+                "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+                "data": "synthetic",
+                "config": {"workload": label, "members": 32, "precision": args.precision,
+                           "form": "one context and stream per member, one time step of each queued in turn",
+                           "sequential_members_substeps_per_s": rate_s,
+                           "l2": "inputs larger than L2 (no flush)"},
+                "finite": ok}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS) + ["c4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
+    if args.config == "c4":
+        return ensemble_main(args)
     cfg = CONFIGS[args.config]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
