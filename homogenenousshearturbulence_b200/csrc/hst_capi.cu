@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "hst_dev.cuh"
 #include "hst_internal.h"
 
 using hst::DeviceState;
@@ -394,7 +395,7 @@ static void free_device(hst_ctx* c) {
   DeviceState& d = c->d;
   for (int i = 0; i < 7; ++i)
     if (d.F[i]) cudaFree(d.F[i]);
-  void* ps[] = {d.Z, d.Pp, d.Q, d.der, d.derS, d.y, d.dyl, d.gdamp, d.twx, d.twz, d.twxf, d.twzf, d.cfl};
+  void* ps[] = {d.Z, d.Pp, d.Q, d.der, d.derS, d.y, d.dyl, d.gdamp, d.twx, d.twz, d.twxf, d.twzf, d.cfl, d.stats};
   for (void* q : ps)
     if (q) cudaFree(q);
   std::memset(&d, 0, sizeof d);
@@ -494,6 +495,8 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   ok = ok && alloc((void**)&d.twz, sizeof(double2) * g.nzd);
   ok = ok && alloc((void**)&d.twxf, sizeof(float2) * 4 * g.nxd);
   ok = ok && alloc((void**)&d.twzf, sizeof(float2) * g.nzd);
+  // outstats scratch (sized for the largest reduction grid, 4 blocks an SM of up to 256 SMs)
+  ok = ok && alloc((void**)&d.stats, sizeof(double) * (13 * 4 * 256 + 8));
   // two words: the CFL maximum and the bounded-wait error flag
   ok = ok && alloc((void**)&d.cfl, 2 * sizeof(unsigned long long));
   if (ok) d.err = reinterpret_cast<int*>(d.cfl + 1);
@@ -752,6 +755,37 @@ extern "C" int hst_gpu_compute_cfl(hst_ctx* ctx, double* cfl) {
   CK(timed(ctx, HST_KC_ZINV, [&] { return hst::launch_zinv(ctx->g, ctx->d, ctx->stream); }));
   CK(timed(ctx, HST_KC_XPROD, [&] { return hst::launch_xprod(ctx->g, ctx->d, ctx->ps, 1, ctx->stream); }));
   return read_cfl(ctx, cfl);
+}
+
+// outstats (src/hst_stats.f90:136-285) of the resident field at `time`:
+// the three DY solves go through RHS1, which is scratch between steps (as
+// the reference's rhs is)
+extern "C" int hst_gpu_outstats(hst_ctx* ctx, double time, double* out) {
+  if (!ctx || !out) return HST_EARG;
+  CK(cudaSetDevice(ctx->device));
+  const Geometry& g = ctx->g;
+  const int nblk = hst::stats_blocks(g, ctx->d.nsm);
+  if (nblk > 4 * 256) return fail(ctx, HST_EARG, "outstats: %d reduction blocks exceed the scratch", nblk);
+  double* pm = ctx->d.stats;
+  double* pg = pm + (size_t)9 * nblk;
+  double* res = pg + (size_t)3 * nblk;
+  double sx, sz;
+  shear_shifts(ctx, time, &sx, &sz);
+  for (int c = 0; c < 3; ++c) {
+    CK(timed(ctx, HST_KC_LINE_SOLVE, [&] {
+      return hst::launch_line_solve(g, ctx->d, ctx->ps, hst::K_DY, 0.0, c, HST_RHS1, sx, sz, ctx->stream);
+    }));
+    CK(hst::launch_stats_grad(g, ctx->d, HST_RHS1, pg + (size_t)c * nblk, ctx->stream));
+    ctx->launches++;
+  }
+  CK(hst::launch_stats_moments(g, ctx->d, ctx->ps, pm, ctx->stream));
+  double ly_w = 0.0;
+  for (int iy = 0; iy < g.ny; ++iy) ly_w += ctx->dyl[iy];
+  CK(hst::launch_stats_final(g, ctx->d, pm, pg, ly_w, ctx->ps.ni, ctx->p.ly, res, ctx->stream));
+  ctx->launches += 2;
+  CK(cudaMemcpyAsync(out, res, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return HST_OK;
 }
 
 // One time step (src/hst_equations.f90:56-87) queued on the stream.

@@ -42,6 +42,9 @@ struct DeviceState {
   // (set by make_transform_maps when the x kernel's 8-point plan uses them)
   CUtensorMap tmZ, tmPp;
   bool maps;
+  int nsm;        // SMs of the device
+  double* stats;  // outstats scratch: block partials of the moments (9 a block), of the three
+                  // gradients (one a block each), then the 8 results
 };
 
 // Scalars of one substep of the column kernel.
@@ -71,6 +74,14 @@ cudaError_t launch_line_solve(const Geometry& g, const DeviceState& d, const Phy
 cudaError_t launch_fill_ghosts(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int field, double sx,
                                double sz, cudaStream_t st);
 size_t column_smem_bytes(const Geometry& g, int exact);
+// outstats (src/hst_stats.f90:136-285): block count of the reductions and
+// the three kernels (hst_stats.cu)
+int stats_blocks(const Geometry& g, int nsm);
+cudaError_t launch_stats_moments(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double* partial,
+                                 cudaStream_t st);
+cudaError_t launch_stats_grad(const Geometry& g, const DeviceState& d, int field, double* partial, cudaStream_t st);
+cudaError_t launch_stats_final(const Geometry& g, const DeviceState& d, const double* pm, const double* pg,
+                               double ly_w, double ni, double ly, double* out, cudaStream_t st);
 // the TMA maps of Z and Pp for the x kernel (d.maps false when not used)
 cudaError_t make_transform_maps(const Geometry& g, DeviceState& d);
 // the stage-ordered twiddles of the 8-point plan of N into out (at most N

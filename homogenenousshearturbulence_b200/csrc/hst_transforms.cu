@@ -372,6 +372,12 @@ typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, v
 
 cudaError_t make_transform_maps(const Geometry& g, DeviceState& d) {
   d.maps = false;
+  {
+    int dev = 0;
+    cudaError_t e0 = cudaGetDevice(&dev);
+    if (e0 == cudaSuccess) e0 = cudaDeviceGetAttribute(&d.nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e0 != cudaSuccess) return e0;
+  }
   if (!xprod_uses_maps(g)) return cudaSuccess;
   void* fn = nullptr;
   cudaDriverEntryPointQueryResult q;

@@ -90,6 +90,7 @@ def lib():
             "hst_gpu_upload_async": (i, [vp, i, vp]),
             "hst_gpu_download_async": (i, [vp, i, vp]),
             "hst_gpu_wait_io": (i, [vp]),
+            "hst_gpu_outstats": (i, [vp, d, P(d)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -356,6 +357,14 @@ class Solver:
     def download_ptr(self, field: int, ptr: int):
         self._check(lib().hst_gpu_download(self._h, field, ct.cast(ct.c_void_p(ptr), ct.POINTER(ct.c_double))),
                     "download")
+
+    def outstats(self, time=None) -> dict:
+        """outstats (src/hst_stats.f90:136-285) on the device: energy,
+        dissipation, uv, vw, uu, vv, ww, uw of the resident field."""
+        t = self.time if time is None else float(time)
+        out = np.zeros(8)
+        self._check(lib().hst_gpu_outstats(self._h, t, out.ctypes.data_as(ct.POINTER(ct.c_double))), "outstats")
+        return dict(zip(["energy", "diss", "uv", "vw", "uu", "vv", "ww", "uw"], out))
 
     def upload_async_ptr(self, field: int, ptr: int):
         """queue the upload of V1..V3 from a pinned host address (see wait_io)"""

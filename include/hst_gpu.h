@@ -154,6 +154,12 @@ int hst_gpu_fill_ghosts_at(hst_ctx* ctx, int field, double time);
  * 163-179): the CFL number of the current V. */
 int hst_gpu_compute_cfl(hst_ctx* ctx, double* cfl);
 
+/* outstats() (src/hst_stats.f90:136-285) of the resident field at `time`:
+ * out[0..7] = energy <u_i u_i>/2, dissipation, uv, vw, uu, vv, ww, uw (box
+ * averages, FP64, a fixed reduction order).  The dissipation's y part
+ * comes from DY solves through HST_RHS1, which is overwritten. */
+int hst_gpu_outstats(hst_ctx* ctx, double time, double* out);
+
 /* device_sync() (src/hst_fft.f90:162) */
 int hst_gpu_sync(hst_ctx* ctx);
 

@@ -428,3 +428,25 @@ def test_mixed_precision_statistics_3000_substeps():
     print("energy", e64, emp, "dissipation", d64, dmp)
     assert abs(emp - e64) <= 5e-3 * abs(e64)
     assert abs(dmp - d64) <= 5e-3 * abs(d64)
+
+
+# ------------------------------------------------------- device outstats ----
+@pytest.mark.parametrize("deck_over", [dict(), dict(nx=63, nz=64, ny=32, exact_shift=True), dict(ystretch=1.5)])
+def test_outstats_matches_oracle(deck_over):
+    """hst_gpu_outstats (src/hst_stats.f90:136-285 on the device) against
+    the oracle's restatement on the same field after 30 substeps: every
+    statistic within 1e-10 relative (of the largest of the eight), and two
+    calls give identical numbers (fixed reduction order)."""
+    deck = c1_deck(**deck_over)
+    V0 = seeded_field(deck, seed=4, k0=4.0, energy=0.1)
+    s, o = make_pair(deck, V0)
+    run_pair(s, o, deck["deltat"], 10)
+    g1 = s.outstats()
+    g2 = s.outstats()
+    r = o.outstats()
+    assert g1 == g2
+    scale = max(abs(v) for v in r.values())
+    for k in r:
+        assert abs(g1[k] - r[k]) <= 1e-10 * scale, (k, g1[k], r[k])
+    assert g1["energy"] > 0 and g1["diss"] > 0
+    s.close()
