@@ -4,6 +4,7 @@
 // reference's host code in the same operation order, so that a Fortran
 // driver that passes its own tables and one that lets the context build them
 // get the same numbers.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -785,6 +786,107 @@ extern "C" int hst_gpu_outstats(hst_ctx* ctx, double time, double* out) {
   ctx->launches += 2;
   CK(cudaMemcpyAsync(out, res, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  return HST_OK;
+}
+
+// ---------------------------------------------------- restart files ----
+// The CPL field file of restart_write / restart_read (src/hst_io.f90:69-178,
+// 240-315): a text header (the mesh with the CPL names: its "ny" is nz and
+// its "nz" is ny+1), raw FP64 time, S, S2, gamma_x, gamma_y, then
+// V(-2..ny+1, -nz..nz, 0..nx) in CPL component order (u, w, v), components
+// innermost; the file's ghost rows are plain copies of rows 0, 1 and
+// ny-2, ny-1.
+static std::string real_txt(double x) {
+  char b[64];
+  std::snprintf(b, sizeof b, "%.17G", x);
+  return b;
+}
+
+extern "C" int hst_gpu_write_restart(hst_ctx* ctx, const char* path, double time, double deltat, double t_max,
+                                     double dt_field, double dt_save) {
+  if (!ctx || !path) return HST_EARG;
+  const hst_gpu_params& p = ctx->p;
+  const Geometry& g = ctx->g;
+  const int ny = g.ny, rows = g.rows;
+  // the three components (FP64, the context's layout)
+  std::vector<double2> V((size_t)3 * g.nf);
+  for (int c = 0; c < 3; ++c) {
+    int rc = hst_gpu_download(ctx, c, reinterpret_cast<double*>(V.data() + (size_t)c * g.nf));
+    if (rc != HST_OK) return rc;
+  }
+  std::string h = "nx=" + std::to_string(p.nx) + " \tny=" + std::to_string(p.nz) + " \tnz=" + std::to_string(ny + 1) +
+                  " \talpha0=" + real_txt(p.alfa0) + " \tbeta0=" + real_txt(p.beta0) +
+                  " \thtcoeff=" + real_txt(p.ystretch > 0.0 ? p.ystretch : -1.0) + " \tRe=" + real_txt(p.re) +
+                  " \tPr=0.71\n" + "deltat=" + real_txt(deltat) + " \tt_max=" + real_txt(t_max) +
+                  " \tdt_field=" + real_txt(dt_field) + " \tdt_save=" + real_txt(dt_save) + "\n" +
+                  "t_field=" + real_txt(time) + "\n" + "meanpx=0 \tmeanflowx=0 \tmeanpy=0 \tmeanflowy=0\n";
+  auto raw = [&](const char* key, double v) {
+    h += key;
+    h += "=\n";
+    h.append(reinterpret_cast<const char*>(&v), 8);
+    h += "\n";
+  };
+  raw("time", time);
+  raw("S", p.S);
+  raw("S2", s2_of(p, time));
+  raw("gamma_x", p.S * time);
+  raw("gamma_y", s2_integral(p, p.s2_start, time));
+  h += "Vfield=\n";
+  FILE* fp = std::fopen(path, "wb");
+  if (!fp) return fail(ctx, HST_EARG, "write_restart: cannot create %s", path);
+  bool ok = std::fwrite(h.data(), 1, h.size(), fp) == h.size();
+  static const int cpl[3] = {0, 2, 1};  // CPL (u, v, w) = (u, w, v) here
+  std::vector<double2> line((size_t)rows * 3);
+  for (int ix = 0; ix < g.nxB && ok; ++ix)
+    for (int iz = 0; iz < g.nzT && ok; ++iz) {
+      const size_t cb = ((size_t)ix * g.nzT + iz) * rows + 2;
+      for (int r = -2; r <= ny + 1; ++r) {
+        const int iy = r < 0 ? r + ny : (r >= ny ? r - ny : r);
+        for (int k = 0; k < 3; ++k) line[(size_t)(r + 2) * 3 + k] = V[(size_t)cpl[k] * g.nf + cb + iy];
+      }
+      ok = std::fwrite(line.data(), sizeof(double2), line.size(), fp) == line.size();
+    }
+  ok = (std::fclose(fp) == 0) && ok;
+  return ok ? HST_OK : fail(ctx, HST_EARG, "write_restart: short write to %s", path);
+}
+
+extern "C" int hst_gpu_read_restart(hst_ctx* ctx, const char* path, double* time) {
+  if (!ctx || !path) return HST_EARG;
+  const Geometry& g = ctx->g;
+  const int ny = g.ny, rows = g.rows;
+  FILE* fp = std::fopen(path, "rb");
+  if (!fp) return fail(ctx, HST_EARG, "read_restart: cannot open %s", path);
+  std::vector<char> all;
+  char b[1 << 16];
+  size_t n;
+  while ((n = std::fread(b, 1, sizeof b, fp)) > 0) all.insert(all.end(), b, b + n);
+  std::fclose(fp);
+  const std::string head(all.begin(), all.begin() + std::min<size_t>(all.size(), 4096));
+  const size_t pv = head.find("Vfield=\n"), pt = head.find("time=\n");
+  if (pv == std::string::npos || pt == std::string::npos) return fail(ctx, HST_EARG, "read_restart: %s has no CPL header", path);
+  auto num = [&](const char* key) -> long {
+    const size_t q = head.find(key);
+    return q == std::string::npos ? -1 : std::strtol(head.c_str() + q + std::strlen(key), nullptr, 10);
+  };
+  if (num("nx=") != ctx->p.nx || num("ny=") != ctx->p.nz || num("nz=") != ny + 1)
+    return fail(ctx, HST_EARG, "read_restart: %s holds another mesh (nx=%ld ny=%ld nz=%ld in CPL names)", path,
+                num("nx="), num("ny="), num("nz="));
+  double t;
+  std::memcpy(&t, all.data() + pt + 6, 8);
+  const size_t need = (size_t)g.nxB * g.nzT * rows * 3 * sizeof(double2);
+  if (all.size() < pv + 8 + need) return fail(ctx, HST_EARG, "read_restart: %s is truncated", path);
+  const char* data = all.data() + pv + 8;
+  static const int cpl[3] = {0, 2, 1};
+  std::vector<double2> V((size_t)g.nf);
+  for (int k = 0; k < 3; ++k) {
+    for (size_t col = 0; col < (size_t)g.ncol; ++col)
+      for (int r = 0; r < rows; ++r)
+        std::memcpy(&V[col * rows + r], data + ((col * rows + r) * 3 + k) * sizeof(double2), sizeof(double2));
+    int rc = hst_gpu_upload(ctx, cpl[k], reinterpret_cast<const double*>(V.data()));
+    if (rc == HST_OK) rc = hst_gpu_fill_ghosts_at(ctx, cpl[k], t);
+    if (rc != HST_OK) return rc;
+  }
+  if (time) *time = t;
   return HST_OK;
 }
 

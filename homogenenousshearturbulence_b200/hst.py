@@ -91,6 +91,8 @@ def lib():
             "hst_gpu_download_async": (i, [vp, i, vp]),
             "hst_gpu_wait_io": (i, [vp]),
             "hst_gpu_outstats": (i, [vp, d, P(d)]),
+            "hst_gpu_write_restart": (i, [vp, ct.c_char_p, d, d, d, d, d]),
+            "hst_gpu_read_restart": (i, [vp, ct.c_char_p, P(d)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -365,6 +367,19 @@ class Solver:
         out = np.zeros(8)
         self._check(lib().hst_gpu_outstats(self._h, t, out.ctypes.data_as(ct.POINTER(ct.c_double))), "outstats")
         return dict(zip(["energy", "diss", "uv", "vw", "uu", "vv", "ww", "uw"], out))
+
+    def write_restart(self, path, deltat=None, t_max=0.0, dt_field=0.0, dt_save=0.0):
+        """restart_write: V in the reference's CPL field file (Dati.cart)."""
+        dt = self.deltat if deltat is None else float(deltat)
+        self._check(lib().hst_gpu_write_restart(self._h, str(path).encode(), self.time, dt, float(t_max),
+                                                float(dt_field), float(dt_save)), "write_restart")
+
+    def read_restart(self, path) -> float:
+        """restart_read of a file of this mesh; sets and returns its time."""
+        t = ct.c_double()
+        self._check(lib().hst_gpu_read_restart(self._h, str(path).encode(), ct.byref(t)), "read_restart")
+        self.time = t.value
+        return t.value
 
     def upload_async_ptr(self, field: int, ptr: int):
         """queue the upload of V1..V3 from a pinned host address (see wait_io)"""

@@ -160,6 +160,17 @@ int hst_gpu_compute_cfl(hst_ctx* ctx, double* cfl);
  * comes from DY solves through HST_RHS1, which is overwritten. */
 int hst_gpu_outstats(hst_ctx* ctx, double time, double* out);
 
+/* restart_write (src/hst_io.f90:240-315): the context's V in the reference's
+ * CPL field file (Dati.cart) at `path`, with deltat, t_max, dt_field and
+ * dt_save in its header text and the raw FP64 time, S, S2(time),
+ * gamma_x = S time and gamma_y(time). */
+int hst_gpu_write_restart(hst_ctx* ctx, const char* path, double time, double deltat, double t_max,
+                          double dt_field, double dt_save);
+/* restart_read (src/hst_io.f90:69-178) of a file of the same mesh: V, with
+ * its ghost rows refilled at the file's time; *time (may be NULL) receives
+ * that time. */
+int hst_gpu_read_restart(hst_ctx* ctx, const char* path, double* time);
+
 /* device_sync() (src/hst_fft.f90:162) */
 int hst_gpu_sync(hst_ctx* ctx);
 
