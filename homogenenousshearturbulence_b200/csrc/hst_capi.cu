@@ -789,6 +789,29 @@ extern "C" int hst_gpu_outstats(hst_ctx* ctx, double time, double* out) {
   return HST_OK;
 }
 
+// compute_pressure (src/hst_pressure.f90:35-110) of the resident field at
+// `time` into field dst (RHS2 in the reference's write_pressure); the
+// transform buffers and RHS1 are scratch
+extern "C" int hst_gpu_pressure(hst_ctx* ctx, double time, int dst) {
+  if (!ctx || dst < HST_OLD1 || dst > HST_RHS2 || dst == HST_RHS1)
+    return fail(ctx, HST_EARG, "pressure: dst must be OLD1, OLD2 or RHS2 (got %d)", dst);
+  CK(cudaSetDevice(ctx->device));
+  const Geometry& g = ctx->g;
+  double sx, sz;
+  shear_shifts(ctx, time, &sx, &sz);
+  CK(timed(ctx, HST_KC_ZINV, [&] { return hst::launch_zinv(g, ctx->d, ctx->stream); }));
+  CK(timed(ctx, HST_KC_XPROD, [&] { return hst::launch_xprod(g, ctx->d, ctx->ps, 0, ctx->stream); }));
+  CK(timed(ctx, HST_KC_ZFWD, [&] { return hst::launch_zfwd(g, ctx->d, ctx->stream); }));
+  CK(hst::launch_pressure_rhs(g, ctx->d, ctx->ps, s2_of(ctx->p, time), sx, sz, ctx->stream));
+  CK(timed(ctx, HST_KC_LINE_SOLVE, [&] {
+    return hst::launch_line_solve(g, ctx->d, ctx->ps, hst::K_POISSON, 0.0, HST_RHS1, dst, sx, sz, ctx->stream);
+  }));
+  CK(hst::launch_pressure_mean(g, ctx->d, ctx->p.ly, dst, ctx->stream));
+  ctx->launches += 2;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return HST_OK;
+}
+
 // ---------------------------------------------------- restart files ----
 // The CPL field file of restart_write / restart_read (src/hst_io.f90:69-178,
 // 240-315): a text header (the mesh with the CPL names: its "ny" is nz and

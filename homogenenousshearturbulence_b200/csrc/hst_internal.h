@@ -82,6 +82,12 @@ cudaError_t launch_stats_moments(const Geometry& g, const DeviceState& d, const 
 cudaError_t launch_stats_grad(const Geometry& g, const DeviceState& d, int field, double* partial, cudaStream_t st);
 cudaError_t launch_stats_final(const Geometry& g, const DeviceState& d, const double* pm, const double* pg,
                                double ly_w, double ni, double ly, double* out, cudaStream_t st);
+// compute_pressure (src/hst_pressure.f90:35-110): the right-hand side into
+// RHS1 (after the transforms), and the (0,0) mode into dst (after the
+// POISSON solve)
+cudaError_t launch_pressure_rhs(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double s2now,
+                                double sx, double sz, cudaStream_t st);
+cudaError_t launch_pressure_mean(const Geometry& g, const DeviceState& d, double ly, int dst, cudaStream_t st);
 // the TMA maps of Z and Pp for the x kernel (d.maps false when not used)
 cudaError_t make_transform_maps(const Geometry& g, DeviceState& d);
 // the stage-ordered twiddles of the 8-point plan of N into out (at most N

@@ -1,4 +1,5 @@
-// The statistics of outstats (src/hst_stats.f90:136-285) on the device:
+// The diagnostics of the resident field on the device: outstats and the
+// pressure.  The statistics of outstats (src/hst_stats.f90:136-285):
 // the box averages of the energy, the dissipation, the Reynolds stresses uv,
 // vw, uw and the variances uu, vv, ww of the resident field, in FP64 with a
 // fixed reduction order (the same result for the same field every time).
@@ -118,6 +119,102 @@ __global__ void k_stats_final(int nblk, const double* __restrict__ pm, const dou
   out[5] = vv * inv;
   out[6] = ww * inv;
   out[7] = uw * inv;
+}
+
+// ------------------------------------------------------------ pressure ----
+// compute_pressure (src/hst_pressure.f90:35-110): the Poisson right-hand
+// side of one row from the six product spectra (their ghost rows the
+// shear-periodic images, as in the right-hand-side kernel) and the
+// mean-shear term -2 i (S alfa + S2 beta) D0 v; the (0,0) column holds
+// -<vv>(y) itself.  One warp per column, lanes over rows.
+template <typename QT>
+__global__ void __launch_bounds__(32 * ST_WARPS) k_pressure_rhs(Geometry g, PhysScalars ps, double s2now, double sx,
+                                                                double sz, const QT* __restrict__ Q,
+                                                                const double2* __restrict__ V2,
+                                                                const double* __restrict__ der,
+                                                                double2* __restrict__ R) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int col = blockIdx.x * ST_WARPS + warp;
+  if (col >= g.ncol) return;
+  const int ny = g.ny;
+  const int ix = col / g.nzT, iz = col - ix * g.nzT - g.nz;
+  const double al = ps.alfa0 * ix, be = ps.beta0 * iz;
+  const cxd ph = cexpi(-(al * sx + be * sz));
+  const size_t qs = (size_t)g.ncol * ny;
+  const QT* Qc = Q + (size_t)col * ny;
+  const double2* Vc = V2 + (size_t)col * g.rows + 2;
+  const double cm = 2.0 * (ps.S * al + s2now * be);
+  for (int r = lane; r < ny; r += 32) {
+    cxd acc = mkc(0, 0);
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+      cxd d0 = mkc(0, 0), d1 = mkc(0, 0), d2 = mkc(0, 0);
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        const int q = r + j - 2;
+        const QT qr = Qc[(size_t)p * qs + (q < 0 ? q + ny : (q >= ny ? q - ny : q))];
+        cxd v = mkc((double)qr.x, (double)qr.y);
+        if (q < 0) v = cmul(v, cconj(ph));
+        if (q >= ny) v = cmul(v, ph);
+        const double e0 = derv(der, ny, r, 0, j - 2), e1 = derv(der, ny, r, 1, j - 2), e2 = derv(der, ny, r, 2, j - 2);
+        d0 = mkc(d0.x + e0 * v.x, d0.y + e0 * v.y);
+        d1 = mkc(d1.x + e1 * v.x, d1.y + e1 * v.y);
+        d2 = mkc(d2.x + e2 * v.x, d2.y + e2 * v.y);
+      }
+      cxd term;
+      if (p == 0) term = cscale(al * al, d0);                           // -(i alfa)^2 d0
+      else if (p == 1) term = cneg(d2);                                 // -d2
+      else if (p == 2) term = cscale(be * be, d0);                      // -(i beta)^2 d0
+      else if (p == 3) term = mkc(2.0 * al * d1.y, -2.0 * al * d1.x);  // -2 i alfa d1
+      else if (p == 4) term = mkc(2.0 * be * d1.y, -2.0 * be * d1.x);  // -2 i beta d1
+      else term = cscale(2.0 * al * be, d0);                            // -2 (i alfa)(i beta) d0
+      if (p == 0) {
+        cxd v0 = mkc(0, 0);
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+          const double e0 = derv(der, ny, r, 0, j - 2);
+          const cxd v = Vc[r + j - 2];
+          v0 = mkc(v0.x + e0 * v.x, v0.y + e0 * v.y);
+        }
+        acc = mkc(term.x + cm * v0.y, term.y - cm * v0.x);  // term - 2 i (S alfa + S2 beta) v0
+      } else {
+        acc = cadd(acc, term);
+      }
+      if (ix == 0 && iz == 0 && p == 1) acc = mkc(-(double)Qc[qs + r].x, 0.0);
+    }
+    R[(size_t)col * g.rows + 2 + r] = acc;
+  }
+}
+
+// the (0,0) mode: p = rhs, its y mean (weights dyl) removed, imaginary part zero
+__global__ void k_pressure_mean(Geometry g, const double2* __restrict__ R, const double* __restrict__ dyl, double ly,
+                                double2* __restrict__ P) {
+  __shared__ double pmean;
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int iy = 0; iy < g.ny; ++iy) s += R[2 + iy].x * dyl[iy];
+    pmean = s / ly;
+  }
+  __syncthreads();
+  for (int iy = threadIdx.x; iy < g.ny; iy += blockDim.x) P[2 + iy] = mkc(R[2 + iy].x - pmean, 0.0);
+}
+
+cudaError_t launch_pressure_rhs(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double s2now,
+                                double sx, double sz, cudaStream_t st) {
+  const int blocks = (g.ncol + ST_WARPS - 1) / ST_WARPS;
+  if (g.mp)
+    k_pressure_rhs<float2><<<blocks, 32 * ST_WARPS, 0, st>>>(g, ps, s2now, sx, sz, reinterpret_cast<const float2*>(d.Q),
+                                                             d.F[1], d.der, d.F[5]);
+  else
+    k_pressure_rhs<double2><<<blocks, 32 * ST_WARPS, 0, st>>>(g, ps, s2now, sx, sz, d.Q, d.F[1], d.der, d.F[5]);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pressure_mean(const Geometry& g, const DeviceState& d, double ly, int dst, cudaStream_t st) {
+  // the (0,0) column is column nz (ix = 0, iz = 0)
+  const size_t c00 = (size_t)g.nz * g.rows;
+  k_pressure_mean<<<1, 256, 0, st>>>(g, d.F[5] + c00, d.dyl, ly, d.F[dst] + c00);
+  return cudaGetLastError();
 }
 
 int stats_blocks(const Geometry& g, int nsm) {

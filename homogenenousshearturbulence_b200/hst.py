@@ -91,6 +91,7 @@ def lib():
             "hst_gpu_download_async": (i, [vp, i, vp]),
             "hst_gpu_wait_io": (i, [vp]),
             "hst_gpu_outstats": (i, [vp, d, P(d)]),
+            "hst_gpu_pressure": (i, [vp, d, i]),
             "hst_gpu_write_restart": (i, [vp, ct.c_char_p, d, d, d, d, d]),
             "hst_gpu_read_restart": (i, [vp, ct.c_char_p, P(d)]),
         }
@@ -367,6 +368,13 @@ class Solver:
         out = np.zeros(8)
         self._check(lib().hst_gpu_outstats(self._h, t, out.ctypes.data_as(ct.POINTER(ct.c_double))), "outstats")
         return dict(zip(["energy", "diss", "uv", "vw", "uu", "vv", "ww", "uw"], out))
+
+    def pressure(self, dst: int = 6, time=None) -> np.ndarray:
+        """compute_pressure (src/hst_pressure.f90:35-110) into field dst
+        (RHS2 by default, as write_pressure); returns that field."""
+        t = self.time if time is None else float(time)
+        self._check(lib().hst_gpu_pressure(self._h, t, int(dst)), "pressure")
+        return self.download(dst)
 
     def write_restart(self, path, deltat=None, t_max=0.0, dt_field=0.0, dt_save=0.0):
         """restart_write: V in the reference's CPL field file (Dati.cart)."""

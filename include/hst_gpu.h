@@ -160,6 +160,14 @@ int hst_gpu_compute_cfl(hst_ctx* ctx, double* cfl);
  * comes from DY solves through HST_RHS1, which is overwritten. */
 int hst_gpu_outstats(hst_ctx* ctx, double time, double* out);
 
+/* compute_pressure (src/hst_pressure.f90:35-110) of the resident field at
+ * `time` into field dst (HST_OLD1, HST_OLD2 or HST_RHS2; the reference's
+ * write_pressure uses rhs(:,:,:,2)): the Poisson right-hand side from the
+ * six products and the mean-shear term, the POISSON solve, the (0,0) mode
+ * -<vv>(y) with zero mean.  RHS1 and the transform buffers are overwritten
+ * (they are scratch between steps). */
+int hst_gpu_pressure(hst_ctx* ctx, double time, int dst);
+
 /* restart_write (src/hst_io.f90:240-315): the context's V in the reference's
  * CPL field file (Dati.cart) at `path`, with deltat, t_max, dt_field and
  * dt_save in its header text and the raw FP64 time, S, S2(time),

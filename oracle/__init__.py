@@ -106,6 +106,7 @@ def lib():
             "ora_start": (None, [vp]),
             "ora_run": (ct.c_long, [vp, ct.c_long]),
             "ora_outstats": (None, [vp, P(d)]),
+            "ora_compute_pressure": (None, [vp, ct.c_int]),
             "ora_restart_write": (i, [vp, ct.c_char_p]),
             "ora_restart_read": (i, [vp, ct.c_char_p]),
             "ora_uniform_from_key": (d, [i, i, i, i, i]),
@@ -288,6 +289,9 @@ class Sim:
         out = np.zeros(8)
         lib().ora_outstats(self.h, out.ctypes.data_as(ct.POINTER(ct.c_double)))
         return dict(zip(["energy", "diss", "uv", "vw", "uu", "vv", "ww", "uw"], out))
+
+    def compute_pressure(self, dst):
+        lib().ora_compute_pressure(self.h, dst)
 
     def restart_write(self, path):
         return lib().ora_restart_write(self.h, str(path).encode())

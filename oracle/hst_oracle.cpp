@@ -1363,6 +1363,66 @@ void ora_outstats(ora_sim* s, double* out) {
   out[7] = uw * inv_ly;
 }
 
+// ------------------------------------------------------------ pressure ----
+// compute_pressure: src/hst_pressure.f90:35-110.  The right-hand side of
+// the pressure Poisson equation from the six product spectra (both groups)
+// and the mean-shear term, into rhs1; the POISSON solve into dst; the (0,0)
+// mode is -<vv> itself with its y mean removed.
+void ora_compute_pressure(ora_sim* s, int dst) {
+  const double s2now = ora_s2_of(s, s->time);
+  const double S = s->p.S;
+  ora_transform_to_physical(s);
+  for (int g = 1; g <= 2; ++g) {
+    ora_build_products(s, g);
+    ora_products_to_spectral(s);
+#pragma omp parallel for
+    for (int ix = 0; ix <= s->nx; ++ix)
+      for (int iz = -s->nz; iz <= s->nz; ++iz) {
+        const cx ialfa = C(0.0, ix * s->p.alfa0), ibeta = C(0.0, iz * s->p.beta0);
+        const int kz = s->izd[iz + s->nz];
+        for (int iy = 0; iy < s->ny; ++iy) {
+          cx r = s->f(ORA_RHS1, iy, iz, ix);
+          for (int p = 1; p <= 3; ++p) {
+            const int m = 3 * (g - 1) + p;
+            cx d0 = C(0, 0), d1 = C(0, 0), d2 = C(0, 0);
+            for (int j = -2; j <= 2; ++j) {
+              cx q = s->vvdz(kz, ix, iy + j, p - 1);
+              d0 = d0 + s->D(iy, 0, j) * q;
+              d1 = d1 + s->D(iy, 1, j) * q;
+              d2 = d2 + s->D(iy, 2, j) * q;
+            }
+            cx term;
+            switch (m) {
+              case 1: term = -((ialfa * ialfa) * d0); break;
+              case 2: term = -d2; break;
+              case 3: term = -((ibeta * ibeta) * d0); break;
+              case 4: term = -((2.0 * ialfa) * d1); break;
+              case 5: term = -((2.0 * ibeta) * d1); break;
+              default: term = -(((2.0 * ialfa) * ibeta) * d0); break;
+            }
+            if (m == 1) {
+              cx v0 = C(0, 0);
+              for (int j = -2; j <= 2; ++j) v0 = v0 + s->D(iy, 0, j) * s->f(ORA_V2, iy + j, iz, ix);
+              r = term - (2.0 * (S * ialfa + s2now * ibeta)) * v0;
+            } else {
+              r = r + term;
+            }
+            if (ix == 0 && iz == 0 && m == 2) r = C(-s->vvdz(0, 0, iy, p - 1).re, 0.0);
+          }
+          s->f(ORA_RHS1, iy, iz, ix) = r;
+        }
+      }
+  }
+  ora_line_solve(s, ORA_POISSON, 0.0, ORA_RHS1, dst, 0, 0, 0);
+  double pmean = 0.0;
+  for (int iy = 0; iy < s->ny; ++iy) {
+    s->f(dst, iy, 0, 0) = s->f(ORA_RHS1, iy, 0, 0);
+    pmean = pmean + s->f(dst, iy, 0, 0).re * s->dyl[iy];
+  }
+  pmean = pmean / s->p.ly;
+  for (int iy = 0; iy < s->ny; ++iy) s->f(dst, iy, 0, 0) = C(s->f(dst, iy, 0, 0).re - pmean, 0.0);
+}
+
 // -------------------------------------------------------- field files ----
 // restart_write / write_cpl: src/hst_io.f90:240-315.  Header as io.cpl
 // writes it; the array (0..nx, -nz..nz, -2..ny+1) of CPL (u, v, w) =

@@ -113,6 +113,8 @@ long ora_run(ora_sim* s, long max_steps);
 /* statistics of src/hst_stats.f90:136-285: out = energy, diss, uv, vw, uu, vv, ww, uw
  * (box means, Runtimedata columns 10-13 and variances_runtime.dat) */
 void ora_outstats(ora_sim* s, double* out);
+/* compute_pressure (src/hst_pressure.f90:35-110) into field dst; rhs1 is scratch */
+void ora_compute_pressure(ora_sim* s, int dst);
 
 /* CPL field files (src/hst_io.f90:240-315, 69-178) */
 int ora_restart_write(ora_sim* s, const char* path);

@@ -483,3 +483,47 @@ def test_restart_files(golden, tmp_path):
     assert np.abs(W - V).max() <= 1e-14 * np.abs(V).max()
     s.close()
     r.close()
+
+
+# ---------------------------------------------------------------- pressure ----
+def test_pressure_taylor_green(golden):
+    """tests/test_pressure.f90 of the reference on the GPU: the Taylor-Green
+    pressure p(2mx, 0) = -1/8, p(0,0)(y) = -cos(2ky)/4 within 1e-4 and every
+    other mode below 1e-10."""
+    from tests.test_oracle_golden import taylor_green_pressure_case
+    deck, o, U, Vv, ky, y = taylor_green_pressure_case(golden, oracle.Sim, deck_to_oracle)
+    s = hst.Solver(deck)
+    s.time = 0.0
+    s.set_velocity(np.stack([U, Vv, np.zeros_like(U)]))
+    p = s.pressure()[..., 2:-2]
+    nz, mx = deck["nz"], 3
+    err = max(np.abs(p[2 * mx, nz] + 0.125).max(), np.abs(p[0, nz] + 0.25 * np.cos(2 * ky * y[2:-2])).max())
+    other = p.copy()
+    other[2 * mx, nz] = 0
+    other[0, nz] = 0
+    assert err <= 1e-4, err
+    assert np.abs(other).max() <= 1e-10
+    s.close()
+
+
+@pytest.mark.parametrize("deck_over,prec,tol", [(dict(), "fp64", 1e-10),
+                                                (dict(nx=63, nz=64, ny=32, s2_amplitude=0.5, s2_period=10.0), "fp64",
+                                                 1e-10),
+                                                (dict(), "mixed", 1e-5)])
+def test_pressure_matches_oracle(deck_over, prec, tol):
+    """hst_gpu_pressure against the oracle's compute_pressure on a seeded
+    field after 30 substeps: relative L2 over the interior rows."""
+    deck = c1_deck(**deck_over)
+    V0 = seeded_field(deck, seed=6, k0=4.0, energy=0.1)
+    s, o = make_pair(dict(deck, precision=prec), V0)
+    run_pair(s, o, deck["deltat"], 10)
+    if prec == "mixed":  # the same field in both (the step itself is tested elsewhere)
+        V = s.velocity()
+        for c in range(3):
+            o.field(c)[...] = V[c]
+    pg = s.pressure()
+    o.compute_pressure(oracle.RHS2)
+    po = o.field(oracle.RHS2).copy()
+    err = rel_l2(pg, po)
+    assert err <= tol, (deck_over, prec, err)
+    s.close()
