@@ -91,12 +91,13 @@ __global__ void k_column(ColumnArgs a) {
   const unsigned gmask = group_mask(P);
   const int mi = g.m - 2;
   const int lineN = P * g.MS;
-  const size_t per_group = (size_t)(EXACT ? 3 : 2) * lineN * 2 + (size_t)mi * 4 * P;  // doubles
+  constexpr int NL = (EXACT && MODE == COL_FUSED) ? 3 : 2;  // lines held
+  const size_t per_group = (size_t)NL * lineN * 2 + (size_t)mi * 4 * P;  // doubles
   double* base = smem_d + per_group * grp;
   cxd* bufA = reinterpret_cast<cxd*>(base);
   cxd* bufB = bufA + lineN;
-  cxd* bufC = bufB + lineN;  // EXACT only
-  double* fac = base + (size_t)(EXACT ? 3 : 2) * lineN * 2;
+  cxd* bufC = bufB + lineN;  // EXACT and COL_FUSED only
+  double* fac = base + (size_t)NL * lineN * 2;
 
   const int ix = col / nzT, iz = col - ix * nzT - nz;
   const bool c00 = (ix == 0 && iz == 0);
@@ -135,50 +136,53 @@ __global__ void k_column(ColumnArgs a) {
     }
   }
   if (MODE == COL_RHS) return;
-  if (MODE == COL_SOLVE) {
-    for (int r = s; r < ny; r += P) {
-      bufA[G.at(r)] = a.R1[cb + r];
-      bufB[G.at(r)] = a.R2[cb + r];
-    }
-  }
-  __syncwarp(gmask);
 
-  if (EXACT) {
-    // shift_unweighted (src/hst_equations.f90:263-293) on rhs1, rhs2, old1,
-    // old2: D0 solve with the wrap at t, node phase, ghost rows at t+dt_sub,
-    // D0 stencil.  The scratch is this column of V1, dead here.
-    const double th0 = al * sc.sx_t + be * sc.sz_t;
-    const cxd ph1 = cexpi(-(al * sc.sx_n + be * sc.sz_n));
-    double2* scr = a.V1 + (size_t)col * g.rows;
-    for (int qi = 0; qi < 4; ++qi) {
-      cxd* X = qi == 0 ? bufA : (qi == 1 ? bufB : bufC);
-      double2* Og = qi == 2 ? a.O1 : a.O2;
-      if (qi >= 2) {
-        for (int r = s; r < ny; r += P) X[G.at(r)] = Og[cb + r];
-        __syncwarp(gmask);
-      }
-      group_solve<P>(K_D0, 0.0, ni, kk, th0, DS, G, X, fac, s, gmask);
-      __syncwarp(gmask);
+  // shift_unweighted (src/hst_equations.f90:263-293) on rhs1, rhs2, old1,
+  // old2 (EXACT): D0 solve with the wrap at t, node phase, ghost rows at
+  // t+dt_sub, D0 stencil.  The scratch is this column of V1, dead here.
+  // The split stage shifts old1 and old2 first, through bufA, then loads
+  // rhs1, rhs2 (step -1), so that it holds two lines, not three.
+  const int nseq = MODE == COL_SOLVE ? (EXACT ? 5 : 1) : (EXACT ? 4 : 0);
+  const double th0 = al * sc.sx_t + be * sc.sz_t;
+  double2* scr = a.V1 + (size_t)col * g.rows;
+#pragma unroll 1
+  for (int k = 0; k < nseq; ++k) {
+    const int qi = MODE == COL_SOLVE ? (EXACT ? (k < 2 ? k + 2 : (k == 2 ? -1 : k - 3)) : -1) : k;
+    if (qi < 0) {
       for (int r = s; r < ny; r += P) {
-        cxd v = cmul(X[G.at(r)], cexpi(-(al * sc.dgx + be * sc.dgz) * a.y[r + 2]));
-        X[G.at(r)] = v;
+        bufA[G.at(r)] = a.R1[cb + r];
+        bufB[G.at(r)] = a.R2[cb + r];
       }
       __syncwarp(gmask);
-      store_with_ghosts<P>(scr, X, G, ny, ph1, s, false);
-      __syncwarp(gmask);
-      for (int r = s; r < ny; r += P) {
-        cxd acc = mkc(0, 0);
-#pragma unroll
-        for (int j = 0; j < 5; ++j) {
-          double d0 = derv(der, ny, r, 0, j - 2);
-          cxd v = scr[r + j];
-          acc = mkc(acc.x + d0 * v.x, acc.y + d0 * v.y);
-        }
-        if (qi >= 2) Og[cb + r] = acc;
-        else X[G.at(r)] = acc;
-      }
+      continue;
+    }
+    cxd* X = qi == 0 ? bufA : (qi == 1 ? bufB : (MODE == COL_SOLVE ? bufA : bufC));
+    double2* Og = qi == 2 ? a.O1 : a.O2;
+    if (qi >= 2) {
+      for (int r = s; r < ny; r += P) X[G.at(r)] = Og[cb + r];
       __syncwarp(gmask);
     }
+    group_solve<P>(K_D0, 0.0, ni, kk, th0, DS, G, X, fac, s, gmask);
+    __syncwarp(gmask);
+    for (int r = s; r < ny; r += P) {
+      cxd v = cmul(X[G.at(r)], cexpi(-(al * sc.dgx + be * sc.dgz) * a.y[r + 2]));
+      X[G.at(r)] = v;
+    }
+    __syncwarp(gmask);
+    store_with_ghosts<P>(scr, X, G, ny, cexpi(-(al * sc.sx_n + be * sc.sz_n)), s, false);
+    __syncwarp(gmask);
+    for (int r = s; r < ny; r += P) {
+      cxd acc = mkc(0, 0);
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        double d0 = derv(der, ny, r, 0, j - 2);
+        cxd v = scr[r + j];
+        acc = mkc(acc.x + d0 * v.x, acc.y + d0 * v.y);
+      }
+      if (qi >= 2) Og[cb + r] = acc;
+      else X[G.at(r)] = acc;
+    }
+    __syncwarp(gmask);
   }
 
   // ---- implicit solves (linsolve, src/hst_equations.f90:298-326)
@@ -431,7 +435,7 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
     return cudaGetLastError();
   }
   // 32 or 64 threads, fewer groups when their shared memory would not fit
-  const size_t per = column_smem_bytes(g, EXACT);
+  const size_t per = column_smem_bytes(g, EXACT && MODE == COL_FUSED);
   int groups = (P >= 32 ? 32 : 64) / P;
   if (groups < 1) groups = 1;
   while (groups > 1 && per * groups > 200 * 1024) groups >>= 1;

@@ -104,10 +104,11 @@ struct ZfwdDst {
 };
 
 // (the explicit one-block minimum lets the compiler take 160 registers
-// here, which measured 0.46 against 0.50 ms at 384^2 x 256; the same on
-// k_zinv measured slower)
+// for the 16-point plans, which measured 0.46 against 0.50 ms at 384^2 x
+// 256; the same on k_zinv measured slower; the 8-point plans are held to
+// two blocks an SM)
 template <int NT, int PPT, typename C>
-__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256, 1) k_zfwd(Geometry g, const C* __restrict__ Pp, C* __restrict__ Q,
+__global__ void __launch_bounds__(PPT <= 8 ? 384 : 256, PPT <= 8 ? 2 : 1) k_zfwd(Geometry g, const C* __restrict__ Pp, C* __restrict__ Q,
                                               const C* __restrict__ twz) {
   extern __shared__ double2 sh_d[];
   C* sh = reinterpret_cast<C*>(sh_d);
