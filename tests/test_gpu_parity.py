@@ -527,3 +527,23 @@ def test_pressure_matches_oracle(deck_over, prec, tol):
     err = rel_l2(pg, po)
     assert err <= tol, (deck_over, prec, err)
     s.close()
+
+
+# ------------------------------------------------- the alternative kernel paths ----
+@pytest.mark.parametrize("env", [dict(HST_COLUMN_FUSED="1"), dict(HST_RHS_TILED="0"), dict(HST_LINE_LANES="16"),
+                                 dict(HST_FFT_PPT_X="16", HST_FFT_PPT_Z="8")])
+@pytest.mark.parametrize("exact", [False, True])
+def test_alternative_paths_parity(monkeypatch, env, exact):
+    """The kernel paths the environment selects (the fused column kernel,
+    the untiled right-hand sides, 16-lane solver groups, the other FFT plan
+    families) against the oracle: 10 substeps of a 192 x 192 x 64 deck
+    (nx = 63, nz = 64, ny = 64), relative L2 <= 1e-12."""
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    deck = c1_deck(nx=63, nz=64, ny=64, exact_shift=exact)
+    V0 = seeded_field(deck, seed=8, k0=6.0, energy=0.1)
+    s, o = make_pair(deck, V0)
+    Vg, Vo = run_pair(s, o, deck["deltat"], 10)
+    err = rel_l2(Vg, Vo)
+    assert err <= 1e-12, (env, exact, err)
+    s.close()
