@@ -547,3 +547,17 @@ def test_alternative_paths_parity(monkeypatch, env, exact):
     err = rel_l2(Vg, Vo)
     assert err <= 1e-12, (env, exact, err)
     s.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("mixed", 1e-5)])
+def test_x_384_parity(prec, tol):
+    """The x kernel at 384 points (the 384^2 workload's 2 nxd) on a narrow
+    deck (nx = 127, nz = 32, ny = 32): 10 substeps against the oracle."""
+    deck = c1_deck(nx=127, nz=32, ny=32)
+    V0 = seeded_field(deck, seed=12, k0=8.0, energy=0.1)
+    s, o = make_pair(dict(deck, precision=prec), V0)
+    assert s.nxd == 192
+    Vg, Vo = run_pair(s, o, deck["deltat"], 10)
+    err = rel_l2(Vg, Vo)
+    assert err <= tol, (prec, err)
+    s.close()
