@@ -812,6 +812,127 @@ extern "C" int hst_gpu_pressure(hst_ctx* ctx, double time, int dst) {
   return HST_OK;
 }
 
+static int queue_timestep(hst_ctx* ctx, double* time, double deltat);
+
+// ------------------------------------------------------------ autotune ----
+// Tries the launch choices that leave every buffer's layout unchanged -- the
+// lanes of a line-solver group (P) and the points a thread of the x and z
+// FFT plans -- on this context's own sizes, `steps` time steps each after
+// one untimed step, keeps the fastest, and puts the fields and the time back
+// as they were.  The report lists every candidate with its time a step.
+extern "C" int hst_gpu_autotune(hst_ctx* ctx, double deltat, int steps, char* report, int report_len) {
+  if (!ctx || steps < 1) return fail(ctx, HST_EARG, "autotune: bad arguments");
+  CK(cudaSetDevice(ctx->device));
+  Geometry& g = ctx->g;
+  const Geometry g0 = g;
+  std::string rep;
+  // state to put back: V1..V3, OLD1, OLD2 (RHS1/2 and the transform buffers are scratch)
+  std::vector<double2*> save(5, nullptr);
+  auto release = [&] {
+    for (double2* q : save)
+      if (q) cudaFree(q);
+  };
+  const size_t fb = sizeof(double2) * g.nf;
+  for (int i = 0; i < 5; ++i) {
+    if (cudaMalloc((void**)&save[i], fb) != cudaSuccess) {
+      cudaGetLastError();
+      release();
+      return fail(ctx, HST_ENOMEM, "autotune: no room for a copy of the state");
+    }
+    CK(cudaMemcpyAsync(save[i], ctx->d.F[i], fb, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  // the damping state the trial steps may move on
+  const double theta0 = ctx->theta_last, time0 = 0.0;
+  const std::vector<double> gdamp0 = ctx->gdamp;
+  // candidates
+  std::vector<int> lanes;
+  for (int c = 32; c >= 4; c >>= 1) {
+    Geometry t = g0;
+    if (g0.ny % c != 0 || g0.ny / c < 4) continue;
+    t.P = c;
+    t.m = g0.ny / c;
+    t.MS = t.m | 1;
+    if (hst::column_smem_bytes(t, 1) <= 200 * 1024) lanes.push_back(c);
+  }
+  const int NX = 2 * g0.nxd;
+  std::vector<int> px, pz;
+  if (g0.mp) {
+    px.push_back(8);
+  } else {
+    px.push_back(16);
+    if (NX == 192 || NX == 384 || NX == 768) px.push_back(8);
+  }
+  for (int v : {16, 8}) {
+    if (g0.mp && g0.nzd == 768 && v == 16) continue;
+    if (v == 8 && !(g0.nzd == 192 || g0.nzd == 384 || g0.nzd == 768)) continue;
+    if (v == 8 && g0.Ty * g0.nzd / 8 > 384) continue;
+    if (v == 16 && g0.Ty * g0.nzd / 16 > 256) continue;
+    pz.push_back(v);
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double best = 1e300;
+  Geometry gbest = g0;
+  int rc = HST_OK;
+  auto apply = [&](const Geometry& t) -> cudaError_t {
+    g = t;
+    auto ds = slab_major(ctx->der, g.ny, g.P, g.m);
+    cudaError_t e = cudaMemcpy(ctx->d.derS, ds.data(), sizeof(double) * 20 * g.ny, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = hst::make_transform_maps(g, ctx->d);
+    return e;
+  };
+  for (int P : lanes)
+    for (int a : px)
+      for (int b : pz) {
+        Geometry t = g0;
+        t.P = P;
+        t.m = g0.ny / P;
+        t.MS = t.m | 1;
+        t.pptx = a;
+        t.pptz = b;
+        if (apply(t) != cudaSuccess) continue;
+        for (int i = 0; i < 5 && rc == HST_OK; ++i)
+          if (cudaMemcpyAsync(ctx->d.F[i], save[i], fb, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+            rc = HST_ECUDA;
+        double tt = time0;
+        if (rc == HST_OK) rc = queue_timestep(ctx, &tt, deltat);
+        if (rc == HST_OK && cudaEventRecord(e0, ctx->stream) != cudaSuccess) rc = HST_ECUDA;
+        for (int k = 0; k < steps && rc == HST_OK; ++k) rc = queue_timestep(ctx, &tt, deltat);
+        if (rc == HST_OK && cudaEventRecord(e1, ctx->stream) != cudaSuccess) rc = HST_ECUDA;
+        if (rc == HST_OK && cudaEventSynchronize(e1) != cudaSuccess) rc = HST_ECUDA;
+        if (rc != HST_OK) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double per = ms / steps;
+        char line[128];
+        std::snprintf(line, sizeof line, "P=%d x=%d z=%d: %.4f ms a step\n", P, a, b, per);
+        rep += line;
+        if (per < best) {
+          best = per;
+          gbest = t;
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // the winner, and the state as it was
+  if (apply(rc == HST_OK ? gbest : g0) != cudaSuccess && rc == HST_OK) rc = HST_ECUDA;
+  for (int i = 0; i < 5; ++i) cudaMemcpyAsync(ctx->d.F[i], save[i], fb, cudaMemcpyDeviceToDevice, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  release();
+  ctx->theta_last = theta0;
+  if (ctx->gdamp != gdamp0) {
+    ctx->gdamp = gdamp0;
+    CK(cudaMemcpy(ctx->d.gdamp, ctx->gdamp.data(), sizeof(double) * g.ncol, cudaMemcpyHostToDevice));
+  }
+  if (rc != HST_OK) return rc;
+  char line[128];
+  std::snprintf(line, sizeof line, "chosen: P=%d x=%d z=%d\n", g.P, g.pptx, g.pptz);
+  rep += line;
+  if (report && report_len > 0) std::snprintf(report, (size_t)report_len, "%s", rep.c_str());
+  return HST_OK;
+}
+
 // ---------------------------------------------------- restart files ----
 // The CPL field file of restart_write / restart_read (src/hst_io.f90:69-178,
 // 240-315): a text header (the mesh with the CPL names: its "ny" is nz and

@@ -92,6 +92,7 @@ def lib():
             "hst_gpu_wait_io": (i, [vp]),
             "hst_gpu_outstats": (i, [vp, d, P(d)]),
             "hst_gpu_pressure": (i, [vp, d, i]),
+            "hst_gpu_autotune": (i, [vp, d, i, ct.c_char_p, i]),
             "hst_gpu_write_restart": (i, [vp, ct.c_char_p, d, d, d, d, d]),
             "hst_gpu_read_restart": (i, [vp, ct.c_char_p, P(d)]),
         }
@@ -368,6 +369,14 @@ class Solver:
         out = np.zeros(8)
         self._check(lib().hst_gpu_outstats(self._h, t, out.ctypes.data_as(ct.POINTER(ct.c_double))), "outstats")
         return dict(zip(["energy", "diss", "uv", "vw", "uu", "vv", "ww", "uw"], out))
+
+    def autotune(self, deltat=None, steps: int = 3) -> str:
+        """Pick the fastest line-solver group width and FFT plans for this
+        context's sizes (the fields are left as they were); returns the report."""
+        dt = self.deltat if deltat is None else float(deltat)
+        buf = ct.create_string_buffer(4096)
+        self._check(lib().hst_gpu_autotune(self._h, dt, int(steps), buf, 4096), "autotune")
+        return buf.value.decode()
 
     def pressure(self, dst: int = 6, time=None) -> np.ndarray:
         """compute_pressure (src/hst_pressure.f90:35-110) into field dst

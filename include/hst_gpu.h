@@ -160,6 +160,15 @@ int hst_gpu_compute_cfl(hst_ctx* ctx, double* cfl);
  * comes from DY solves through HST_RHS1, which is overwritten. */
 int hst_gpu_outstats(hst_ctx* ctx, double time, double* out);
 
+/* Tries the launch choices that keep every buffer's layout -- the lanes of
+ * a line-solver group and the points a thread of the x and z FFT plans --
+ * on this context's sizes (`steps` time steps of `deltat` each, after one
+ * untimed step), keeps the fastest and restores the fields (V, OLD) and
+ * the damping state.  A report of the candidates' times a step goes to
+ * report[0:report_len) when report is not NULL.  It allocates a copy of
+ * five fields while it runs.  No counterpart in the reference. */
+int hst_gpu_autotune(hst_ctx* ctx, double deltat, int steps, char* report, int report_len);
+
 /* compute_pressure (src/hst_pressure.f90:35-110) of the resident field at
  * `time` into field dst (HST_OLD1, HST_OLD2 or HST_RHS2; the reference's
  * write_pressure uses rhs(:,:,:,2)): the Poisson right-hand side from the

@@ -561,3 +561,22 @@ def test_x_384_parity(prec, tol):
     err = rel_l2(Vg, Vo)
     assert err <= tol, (prec, err)
     s.close()
+
+
+# ------------------------------------------------------------------ autotune ----
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("mixed", 1e-5)])
+def test_autotune_keeps_state_and_parity(prec, tol):
+    """hst_gpu_autotune tries the layout-neutral launch choices, leaves the
+    fields exactly as they were, and the chosen configuration still matches
+    the oracle over 10 substeps."""
+    deck = c1_deck(nx=63, nz=64, ny=64, exact_shift=True)
+    V0 = seeded_field(deck, seed=13, k0=6.0, energy=0.1)
+    s, o = make_pair(dict(deck, precision=prec), V0)
+    before = s.velocity()
+    rep = s.autotune(deck["deltat"], steps=2)
+    assert "chosen:" in rep and rep.count("ms a step") >= 2
+    assert np.array_equal(s.velocity(), before)
+    Vg, Vo = run_pair(s, o, deck["deltat"], 10)
+    err = rel_l2(Vg, Vo)
+    assert err <= tol, (prec, err, rep)
+    s.close()
