@@ -82,3 +82,18 @@ def test_async_io_and_noalloc_reject_bad_arguments():
     assert f(15, 4096, 15, 1.0, 1.0, 100.0, 1, 1.0, 16, 32, 64, 0.0, 0.0, None, msg, 128) == -1
     assert b"scratch" in msg.value
     assert f(15, 31, 15, 1.0, 1.0, 100.0, 1, 1.0, 16, 32, 64, 0.0, 0.0, None, msg, 128) == -1
+
+
+def test_mixed_precision_rejects_uncompiled_sizes():
+    """HST_PREC_MIXED needs 2 nxd and nzd in {96, 192, 384, 768} and ny a
+    multiple of 32; anything else is refused before any CUDA call."""
+    for nx, ny, nz in ((15, 32, 15), (31, 48, 32), (31, 64, 20)):
+        p = hst.Params()
+        p.nx, p.ny, p.nz = nx, ny, nz
+        p.alfa0, p.beta0, p.ly, p.re = 1.0, 1.0, 2.0, 100.0
+        p.precision = hst.PREC_MIXED
+        h = ct.c_void_p()
+        assert hst.lib().hst_gpu_create(ct.byref(p), ct.byref(h)) == -1 and not h.value
+        assert hst.lib().hst_gpu_device_bytes(ct.byref(p)) == 0.0
+    p.precision = 7
+    assert hst.lib().hst_gpu_device_bytes(ct.byref(p)) == 0.0

@@ -580,3 +580,17 @@ def test_autotune_keeps_state_and_parity(prec, tol):
     err = rel_l2(Vg, Vo)
     assert err <= tol, (prec, err, rep)
     s.close()
+
+
+@pytest.mark.parametrize("sizes", [dict(nx=7, nz=5, ny=16), dict(nx=2, nz=1, ny=8), dict(nx=21, nz=10, ny=24)])
+def test_small_and_uneven_sizes(sizes):
+    """Sizes off the compiled paths: transform lengths of the runtime FFT
+    plan (16, 6), two-lane solver groups (ny = 8, 16) and ny not a multiple
+    of 32 (the untiled right-hand sides): 10 substeps against the oracle."""
+    deck = c1_deck(**sizes)
+    V0 = seeded_field(deck, seed=14, k0=2.0, energy=0.1)
+    s, o = make_pair(deck, V0)
+    Vg, Vo = run_pair(s, o, deck["deltat"], 10)
+    err = rel_l2(Vg, Vo)
+    assert err <= 1e-12, (sizes, err)
+    s.close()
