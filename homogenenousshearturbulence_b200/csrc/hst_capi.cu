@@ -336,13 +336,15 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
   }
   if (g.mp) {
     if (!hst::mp_length_ok(2 * g.nxd) || !hst::mp_length_ok(g.nzd) || p.ny % 32 != 0) {
-      why = "mixed precision needs 2 nxd and nzd in {96, 192, 384, 768} and ny a multiple of 32";
+      why = "mixed precision needs 2 nxd and nzd in {96, 192, 384, 768, 1536} and ny a multiple of 32";
       return HST_EARG;
     }
     g.pptx = 8;
     // 16 points a thread for the FP32 z transforms (zfwd 0.29 against 0.34 ms at 384)
     g.pptz = g.nzd == 768 ? 8 : ppt_of("HST_FFT_PPT_Z", 16);
   }
+  // 1536 points: one plan in both precisions, 32 points a thread
+  if (g.nzd == 1536) g.pptz = 32;
   // transform y tile (at most 512 threads for the 8-point z plans)
   g.Ty = 2;
   for (int t : {8, 4}) {
@@ -869,6 +871,7 @@ extern "C" int hst_gpu_autotune(hst_ctx* ctx, double deltat, int steps, char* re
     if (v == 16 && g0.Ty * g0.nzd / 16 > 256) continue;
     pz.push_back(v);
   }
+  if (pz.empty()) pz.push_back(g0.pptz);  // one plan only (1536 points)
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));

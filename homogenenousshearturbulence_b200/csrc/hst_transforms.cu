@@ -438,7 +438,8 @@ static void big_smem(K k) {
   } while (0)
 
 // The mixed-precision form compiles the transforms for the lengths its
-// workloads use: 8 points a thread at 192, 384 and 768, 16 at 96.
+// workloads use: 8 points a thread at 192, 384 and 768, 16 at 96, 32 (the
+// radix 16, 16, 6 plan) at 1536.
 #define HST_FFT_DISPATCH_MP(N, P16, CALL)          \
   do {                                             \
     switch (N) {                                   \
@@ -448,12 +449,13 @@ static void big_smem(K k) {
       case 384:                                    \
         if (P16) CALL(384, 16) else CALL(384, 8) break; \
       case 768: CALL(768, 8) break;                \
+      case 1536: CALL(1536, 32) break;             \
       default:                                     \
         return cudaErrorInvalidValue;              \
     }                                              \
   } while (0)
 
-bool mp_length_ok(int n) { return n == 96 || n == 192 || n == 384 || n == 768; }
+bool mp_length_ok(int n) { return n == 96 || n == 192 || n == 384 || n == 768 || n == 1536; }
 
 cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st) {
   const int pts = g.nzd * g.Ty;

@@ -453,9 +453,15 @@ def random_field(nx, ny, nz, alfa0, beta0, ly, y, seed=1, k0=4.0, energy=0.1, en
     field is rescaled so that <u_i u_i>/2 = energy (box mean, as
     src/hst_stats.f90:257-269 reports it).  Returns (3, nx+1, 2nz+1, ny+4)."""
     mmax = ny // 3
-    ix = np.arange(nx + 1)[:, None, None]
-    iz = np.arange(-nz, nz + 1)[None, :, None]
-    m = np.arange(-mmax, mmax + 1)[None, None, :]
+    # both envelopes are below their 1e-8 cut beyond k = 5 k0, so only the
+    # modes of that box are drawn (the 1536^2 x 512 field in seconds)
+    kcut = 5.0 * k0
+    nxb = min(nx, int(kcut / abs(alfa0)))
+    nzb = min(nz, int(kcut / abs(beta0)))
+    mb = min(mmax, int(kcut * ly / (2.0 * PI)))
+    ix = np.arange(nxb + 1)[:, None, None]
+    iz = np.arange(-nzb, nzb + 1)[None, :, None]
+    m = np.arange(-mb, mb + 1)[None, None, :]
     kx = alfa0 * ix
     kz = beta0 * iz
     ky = 2.0 * PI * m / ly
@@ -463,7 +469,7 @@ def random_field(nx, ny, nz, alfa0, beta0, ly, y, seed=1, k0=4.0, energy=0.1, en
     q = k / k0
     with np.errstate(divide="ignore", invalid="ignore"):
         env = np.exp(-q * q) if envelope == "gauss" else q * q * np.exp(1.0 - q * q)
-    env = np.where((k == 0.0) | (env < 1e-8), 0.0, env)
+    env = np.where((k == 0.0) | (env < 1e-8) | (q > 5.0), 0.0, env)
     env = np.where((ix == 0) & (iz == 0), 0.0, env)
     mirror = (ix == 0) & ((iz < 0) | ((iz == 0) & (m < 0)))
     jz = np.where(mirror, -iz, iz)
@@ -473,11 +479,25 @@ def random_field(nx, ny, nz, alfa0, beta0, ly, y, seed=1, k0=4.0, energy=0.1, en
         r = uniform_from_key(seed, c, jm, jz, ix)
         ph = 2.0 * PI * uniform_from_key(seed, c + 3, jm, jz, ix)
         ac = r * np.exp(1j * ph)
+        del r, ph
         a.append(np.where(mirror, np.conj(ac), ac) * amplitude * env)
+        del ac
+    del k, q, env, mirror, jz, jm
     I = 1j
-    u = [I * (ky * a[2] - kz * a[1]), I * (kz * a[0] - kx * a[2]), I * (kx * a[1] - ky * a[0])]
-    E = np.exp(I * ky[0, 0, :, None] * y[None, :])  # (nm, ny+4)
-    V = np.stack([np.einsum("xzm,my->xzy", uc, E) for uc in u])
+    E = np.exp(I * ky[0, 0, :, None] * y[None, :])  # (modes in y, ny+4)
+    # one velocity component at a time, projected on the y grid by one
+    # complex matrix product; the modes outside the box stay zero
+    V = np.zeros((3, nx + 1, 2 * nz + 1, len(y)), np.complex128)
+    for c in range(3):
+        if c == 0:
+            uc = I * (ky * a[2] - kz * a[1])
+        elif c == 1:
+            uc = I * (kz * a[0] - kx * a[2])
+        else:
+            uc = I * (kx * a[1] - ky * a[0])
+        V[c, :nxb + 1, nz - nzb:nz + nzb + 1] = (uc.reshape(-1, E.shape[0]) @ E).reshape(nxb + 1, 2 * nzb + 1, len(y))
+        del uc
+    del a
     if energy is not None:
         e = box_energy(V, ly, y)
         if e > 0:
@@ -491,5 +511,7 @@ def box_energy(V, ly, y):
     dyl = 0.5 * (y[3:ny + 3] - y[1:ny + 1])
     w = np.full(V.shape[1], 2.0)
     w[0] = 1.0
-    q = (np.abs(V[:, :, :, 2:ny + 2]) ** 2 * w[None, :, None, None] * dyl[None, None, None, :]).sum()
+    q = 0.0
+    for c in range(V.shape[0]):  # a component at a time: bounded temporaries at large sizes
+        q += float((np.abs(V[c, :, :, 2:ny + 2]) ** 2 * w[:, None, None] * dyl[None, None, :]).sum())
     return 0.5 * q / ly

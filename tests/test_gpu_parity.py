@@ -594,3 +594,22 @@ def test_small_and_uneven_sizes(sizes):
     err = rel_l2(Vg, Vo)
     assert err <= 1e-12, (sizes, err)
     s.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("mixed", 1e-5)])
+@pytest.mark.parametrize("axis", ["x", "z"])
+def test_1536_parity(prec, tol, axis):
+    """The 1536-point transforms of the 1536^2 x 512 workload (2 nxd = 1536
+    from nx = 511; nzd = 1536 from nz = 512) on narrow decks, with that
+    workload's exact_shift, oscillating S2 (0.5 sin(2 pi t / 10)) and hard
+    large-scale damping: 3 time steps against the oracle."""
+    sizes = dict(nx=511, nz=32) if axis == "x" else dict(nx=31, nz=512)
+    deck = c1_deck(ny=32, re=10000.0, deltat=0.0005, exact_shift=True, s2_amplitude=0.5, s2_period=10.0,
+                   damp_kpar=2.0, damp_kperp=2.0, damp_hard=True, time=0.3, **sizes)
+    V0 = seeded_field(deck, seed=15, k0=6.0, energy=0.1)
+    s, o = make_pair(dict(deck, precision=prec), V0)
+    assert (2 * s.nxd if axis == "x" else s.nzd) == 1536
+    Vg, Vo = run_pair(s, o, deck["deltat"], 3)
+    err = rel_l2(Vg, Vo)
+    assert err <= tol, (prec, axis, err)
+    s.close()
