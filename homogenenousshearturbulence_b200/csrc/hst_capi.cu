@@ -398,7 +398,7 @@ static void free_device(hst_ctx* c) {
   DeviceState& d = c->d;
   for (int i = 0; i < 7; ++i)
     if (d.F[i]) cudaFree(d.F[i]);
-  void* ps[] = {d.Z, d.Pp, d.Q, d.der, d.derS, d.y, d.dyl, d.gdamp, d.twx, d.twz, d.twxf, d.twzf, d.cfl, d.stats};
+  void* ps[] = {d.Z, d.Pp, d.Q, d.der, d.derS, d.d0tab, d.y, d.dyl, d.gdamp, d.twx, d.twz, d.twxf, d.twzf, d.cfl, d.stats};
   for (void* q : ps)
     if (q) cudaFree(q);
   std::memset(&d, 0, sizeof d);
@@ -491,6 +491,7 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   ok = ok && alloc((void**)&d.Q, es * 6 * (size_t)g.ncol * g.ny);
   ok = ok && alloc((void**)&d.der, sizeof(double) * 20 * (size_t)ny);
   ok = ok && alloc((void**)&d.derS, sizeof(double) * 20 * (size_t)ny);
+  ok = ok && alloc((void**)&d.d0tab, sizeof(double) * hst::d0_table_doubles(ny));
   ok = ok && alloc((void**)&d.y, sizeof(double) * (ny + 4));
   ok = ok && alloc((void**)&d.dyl, sizeof(double) * ny);
   ok = ok && alloc((void**)&d.gdamp, sizeof(double) * g.ncol);
@@ -520,9 +521,11 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   cudaMemsetAsync(d.cfl, 0, 2 * sizeof(unsigned long long), ctx->stream);
   auto tx = twiddles(2 * g.nxd), tz = twiddles(g.nzd);
   cudaMemcpy(d.der, ctx->der.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice);
+  cudaError_t etab;
   {
     auto ds = slab_major(ctx->der, ny, g.P, g.m);
     cudaMemcpy(d.derS, ds.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice);
+    etab = hst::launch_d0_table(g, d, ctx->stream);
   }
   cudaMemcpy(d.y, ctx->y.data(), sizeof(double) * (ny + 4), cudaMemcpyHostToDevice);
   cudaMemcpy(d.dyl, ctx->dyl.data(), sizeof(double) * ny, cudaMemcpyHostToDevice);
@@ -546,7 +549,8 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
     cudaMemcpy(d.twzf, fz.data(), sizeof(float2) * fz.size(), cudaMemcpyHostToDevice);
   }
   cudaMemcpy(d.twz, tz.data(), sizeof(double2) * tz.size(), cudaMemcpyHostToDevice);
-  cudaError_t e = hst::set_fft_constants();
+  cudaError_t e = etab;
+  if (e == cudaSuccess) e = hst::set_fft_constants();
   if (e == cudaSuccess) e = hst::make_transform_maps(g, d);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -595,6 +599,7 @@ extern "C" int hst_gpu_set_tables(hst_ctx* ctx, const double* der, const double*
     CK(cudaMemcpy(ctx->d.der, ctx->der.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice));
     auto ds = slab_major(ctx->der, ny, ctx->g.P, ctx->g.m);
     CK(cudaMemcpy(ctx->d.derS, ds.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice));
+    CK(hst::launch_d0_table(ctx->g, ctx->d, ctx->stream));
   }
   if (y) {
     std::memcpy(ctx->y.data(), y, sizeof(double) * (ny + 4));
@@ -882,6 +887,7 @@ extern "C" int hst_gpu_autotune(hst_ctx* ctx, double deltat, int steps, char* re
     g = t;
     auto ds = slab_major(ctx->der, g.ny, g.P, g.m);
     cudaError_t e = cudaMemcpy(ctx->d.derS, ds.data(), sizeof(double) * 20 * g.ny, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = hst::launch_d0_table(g, ctx->d, ctx->stream);
     if (e == cudaSuccess) e = hst::make_transform_maps(g, ctx->d);
     return e;
   };

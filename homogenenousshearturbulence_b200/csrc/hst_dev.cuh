@@ -458,4 +458,261 @@ __device__ void group_solve(int sys, double lambda, double ni, double kk, double
   }
 }
 
+// ------------------------------------- the D0 system, factored once ----
+// The matrix of KIND_D0 and KIND_DY (the compact D0 operator) is the same
+// for every Fourier column; only the wrap phase differs.  d0_factor runs the
+// matrix half of group_solve once per context and keeps, per lane s of the
+// group, every matrix quantity that the right-hand side meets: per interior
+// row the two elimination multipliers, the pivot reciprocal, the record
+// weights w, v and the back-substitution factors; the border-row
+// coefficients; each reduction level's two 2x2 blocks; the blocks of the
+// last level.  group_solve_d0 then runs only the right-hand-side half, the
+// same operations in the same order as group_solve, so that the divisions,
+// the block inverses and all matrix shuffles leave every column's
+// dependency chain.  Field f of lane s sits at tab[f P + s].
+__host__ __device__ constexpr int d0_levels(int P) {
+  int n = 0;
+  for (int d = 1; 2 * d < P; d <<= 1) ++n;
+  return n;
+}
+__host__ __device__ constexpr int d0_fields(int m, int P) { return 9 * (m - 2) + 7 + 8 * d0_levels(P) + 24; }
+
+template <int P>
+__device__ void d0_factor(const SlabDer& DS, int m, int s, unsigned gmask, double* __restrict__ tab) {
+  const int mi = m - 2;
+  auto put = [&](int f, double v) { tab[(size_t)f * P + s] = v; };
+  double u11 = 0, u12 = 0, p1 = 0, q1 = 0, u21 = 0, u22 = 0, p2 = 0, q2 = 0;
+  double w1 = 0, w2 = 0, v1 = 0, v2 = 0, sp0 = 0, sq0 = 0, sp1 = 0, sq1 = 0;
+  for (int i = 0; i < mi; ++i) {
+    double a[5];
+    row_coefs(K_D0, 0.0, 0.0, 0.0, DS, s, i, a);
+    double p = 0, q = 0, l0 = 0, l1 = 0;
+    if (i == 0) {
+      p = a[0];
+      q = a[1];
+    }
+    if (i == 1) q = a[0];
+    if (i >= 2) {
+      l0 = a[0];
+      a[1] = a[1] - l0 * u21;
+      a[2] = a[2] - l0 * u22;
+      p = p - l0 * p2;
+      q = q - l0 * q2;
+    }
+    if (i >= 1) {
+      l1 = a[1];
+      a[2] = a[2] - l1 * u11;
+      a[3] = a[3] - l1 * u12;
+      p = p - l1 * p1;
+      q = q - l1 * q1;
+    }
+    const double rp = 1.0 / a[2];
+    const double t1 = a[3] * rp, t2 = a[4] * rp;
+    p = p * rp;
+    q = q * rp;
+    const double w = (i == 0) ? 1.0 : -(u11 * w1 + u22 * w2);
+    const double v = (i == 1) ? 1.0 : -(u11 * v1 + u22 * v2);
+    put(9 * i + 0, l0);
+    put(9 * i + 1, l1);
+    put(9 * i + 2, rp);
+    put(9 * i + 3, w);
+    put(9 * i + 4, v);
+    put(9 * i + 5, t1);
+    put(9 * i + 6, t2);
+    put(9 * i + 7, p);
+    put(9 * i + 8, q);
+    sp0 = sp0 + w * p;
+    sq0 = sq0 + w * q;
+    sp1 = sp1 + v * p;
+    sq1 = sq1 + v * q;
+    w2 = w1;
+    w1 = w;
+    v2 = v1;
+    v1 = v;
+    u21 = u11;
+    u22 = u12;
+    p2 = p1;
+    q2 = q1;
+    u11 = t1;
+    u12 = t2;
+    p1 = p;
+    q1 = q;
+  }
+  const double R3 = sp0, R4 = sq0, R5 = w2 * u22 + w1 * u11, R6 = w1 * u12;
+  const double R9 = sp1, R10 = sq1, R11 = v2 * u22 + v1 * u11, R12 = v1 * u12;
+  const double R15 = p2 - u21 * p1, R16 = q2 - u21 * q1, R17 = u22 - u21 * u11, R18 = -u21 * u12;
+  const double R21 = p1, R22 = q1, R23 = u11, R24 = u12;
+  const int t = (s + 1) & (P - 1);
+  const double T3 = shfl_d(gmask, R3, t, P), T4 = shfl_d(gmask, R4, t, P), T5 = shfl_d(gmask, R5, t, P),
+               T6 = shfl_d(gmask, R6, t, P), T9 = shfl_d(gmask, R9, t, P), T10 = shfl_d(gmask, R10, t, P),
+               T11 = shfl_d(gmask, R11, t, P), T12 = shfl_d(gmask, R12, t, P);
+  double ab1[5], ab2[5];
+  row_coefs(K_D0, 0.0, 0.0, 0.0, DS, s, mi, ab1);
+  row_coefs(K_D0, 0.0, 0.0, 0.0, DS, s, mi + 1, ab2);
+  const double c1m4 = ab1[0], c1m3 = ab1[1], d11 = ab1[2], d12 = ab1[3], c10 = ab1[4];
+  const double c2m3 = ab2[0], d21 = ab2[1], d22 = ab2[2], c20 = ab2[3], c21 = ab2[4];
+  const int B = 9 * mi;
+  put(B + 0, u21);
+  put(B + 1, c1m4);
+  put(B + 2, c1m3);
+  put(B + 3, c10);
+  put(B + 4, c2m3);
+  put(B + 5, c20);
+  put(B + 6, c21);
+  M2 L = {-(c1m4 * R15 + c1m3 * R21), -(c1m4 * R16 + c1m3 * R22), -(c2m3 * R21), -(c2m3 * R22)};
+  M2 D = {d11 - (c1m4 * R17 + c1m3 * R23) - c10 * T3, d12 - (c1m4 * R18 + c1m3 * R24) - c10 * T4,
+          d21 - c2m3 * R23 - (c20 * T3 + c21 * T9), d22 - c2m3 * R24 - (c20 * T4 + c21 * T10)};
+  M2 U = {-(c10 * T5), -(c10 * T6), -(c20 * T5 + c21 * T11), -(c20 * T6 + c21 * T12)};
+  auto put2 = [&](int f, M2 x) {
+    put(f, x.a);
+    put(f + 1, x.b);
+    put(f + 2, x.c);
+    put(f + 3, x.d);
+  };
+  int f = B + 7;
+  for (int d = 1; 2 * d < P; d <<= 1, f += 8) {
+    const int sm = (s - d) & (P - 1), sp = (s + d) & (P - 1);
+    M2 Lm = shfl_m2(gmask, L, sm, P), Dm = shfl_m2(gmask, D, sm, P), Um = shfl_m2(gmask, U, sm, P);
+    M2 Lp = shfl_m2(gmask, L, sp, P), Dp = shfl_m2(gmask, D, sp, P), Up = shfl_m2(gmask, U, sp, P);
+    M2 A = m2mul(L, m2inv(Dm));
+    M2 Gm = m2mul(U, m2inv(Dp));
+    M2 Ln = m2neg(m2mul(A, Lm));
+    M2 Un = m2neg(m2mul(Gm, Up));
+    M2 Dn = m2sub(m2sub(D, m2mul(A, Um)), m2mul(Gm, Lp));
+    put2(f, A);
+    put2(f + 4, Gm);
+    L = Ln;
+    U = Un;
+    D = Dn;
+  }
+  const int q = s ^ (P >> 1);
+  put2(f, L);
+  put2(f + 4, U);
+  put2(f + 8, shfl_m2(gmask, L, q, P));
+  put2(f + 12, shfl_m2(gmask, U, q, P));
+  put2(f + 16, m2inv(shfl_m2(gmask, D, q, P)));
+  put2(f + 20, D);
+}
+
+// group_solve for the D0 matrix from the table of d0_factor, on NR lines
+// at once (buf[k] each as group_solve's buf): the lines share every table
+// load and run as independent dependency chains
+template <int P, int NR>
+__device__ void group_solve_d0(double theta, const double* __restrict__ tab, const LineGeom& G, cxd* const* buf,
+                               int s, unsigned gmask) {
+  const int m = G.m, mi = m - 2, MS = G.MS;
+  auto T = [&](int f) { return __ldg(tab + (size_t)f * P + s); };
+  auto T2 = [&](int f) { return M2{T(f), T(f + 1), T(f + 2), T(f + 3)}; };
+  cxd* sb[NR];
+  cxd x1[NR], x2[NR], sx0[NR], sx1[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    sb[k] = buf[k] + s * MS;
+    x1[k] = x2[k] = sx0[k] = sx1[k] = mkc(0, 0);
+  }
+#pragma unroll 2
+  for (int i = 0; i < mi; ++i) {
+    const double l0 = T(9 * i + 0), l1 = T(9 * i + 1), rp = T(9 * i + 2), w = T(9 * i + 3), v = T(9 * i + 4);
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      cxd bx = sb[k][i];
+      if (i >= 2) bx = cfms(bx, l0, x2[k]);
+      if (i >= 1) bx = cfms(bx, l1, x1[k]);
+      bx = cscale(rp, bx);
+      sb[k][i] = bx;
+      sx0[k] = mkc(sx0[k].x + w * bx.x, sx0[k].y + w * bx.y);
+      sx1[k] = mkc(sx1[k].x + v * bx.x, sx1[k].y + v * bx.y);
+      x2[k] = x1[k];
+      x1[k] = bx;
+    }
+  }
+  const int B = 9 * mi;
+  const double u21 = T(B);
+  const double c1m4 = T(B + 1), c1m3 = T(B + 2), c10 = T(B + 3), c2m3 = T(B + 4), c20 = T(B + 5), c21 = T(B + 6);
+  const int t = (s + 1) & (P - 1);
+  const cxd ph = cexpi(-theta);
+  const cxd mu = cexpi(-(theta / (double)P));
+  cxd mus = mkc(1.0, 0.0);
+  {
+    cxd b = mu;
+    for (int e = s; e; e >>= 1) {
+      if (e & 1) mus = cmul(mus, b);
+      b = cmul(b, b);
+    }
+  }
+  const cxd php = (s == P - 1) ? ph : mkc(1.0, 0.0);
+  V2c r[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    const cxd XM2 = csub(x2[k], cscale(u21, x1[k]));
+    const cxd XM1 = x1[k];
+    const cxd RB1 = sb[k][mi], RB2 = sb[k][mi + 1];
+    const cxd TX0 = shfl_c(gmask, sx0[k], t, P), TX1 = shfl_c(gmask, sx1[k], t, P);
+    cxd b1 = csub(csub(csub(RB1, cscale(c1m4, XM2)), cscale(c1m3, XM1)), cmul(cscale(c10, php), TX0));
+    cxd b2 = csub(csub(RB2, cscale(c2m3, XM1)),
+                  cmul(php, mkc(c20 * TX0.x + c21 * TX1.x, c20 * TX0.y + c21 * TX1.y)));
+    V2c rr = {b1, b2};
+    r[k] = v2scale(cconj(mus), rr);
+  }
+  cxd mud = mu;
+  int f = B + 7;
+#pragma unroll
+  for (int d = 1; 2 * d < P; d <<= 1, f += 8) {
+    const int sm = (s - d) & (P - 1), sp = (s + d) & (P - 1);
+    const M2 A = T2(f), Gm = T2(f + 4);
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      V2c rm = shfl_v2(gmask, r[k], sm, P), rpv = shfl_v2(gmask, r[k], sp, P);
+      V2c ta = v2scale(cconj(mud), m2vec(A, rm));
+      V2c tg = v2scale(mud, m2vec(Gm, rpv));
+      r[k] = v2sub(v2sub(r[k], ta), tg);
+    }
+    mud = cmul(mud, mud);
+  }
+  const C2 Mx = c2_axpby(T2(f), cconj(mud), T2(f + 4), mud);
+  const C2 Mq = c2_axpby(T2(f + 8), cconj(mud), T2(f + 12), mud);
+  const C2 X = c2mul_cr(Mx, T2(f + 16));
+  C2 Sc = c2mul(X, Mq);
+  {
+    const C2 Dc = c2_from(T2(f + 20));
+    Sc.a = csub(Dc.a, Sc.a);
+    Sc.b = csub(Dc.b, Sc.b);
+    Sc.c = csub(Dc.c, Sc.c);
+    Sc.d = csub(Dc.d, Sc.d);
+  }
+  const int q = s ^ (P >> 1);
+  const int sb_ = (s - 1) & (P - 1);
+  cxd xk1[NR], xk2[NR], yb1[NR], yb2[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    V2c rq = shfl_v2(gmask, r[k], q, P);
+    V2c rhs = v2sub(r[k], c2vec(X, rq));
+    const V2c c = c2solve(Sc, rhs);
+    const cxd xb1 = cmul(mus, c.u), xb2 = cmul(mus, c.v);
+    yb1[k] = shfl_c(gmask, xb1, sb_, P);
+    yb2[k] = shfl_c(gmask, xb2, sb_, P);
+    if (s == 0) {
+      yb1[k] = cmul(cconj(ph), yb1[k]);
+      yb2[k] = cmul(cconj(ph), yb2[k]);
+    }
+    sb[k][mi] = xb1;
+    sb[k][mi + 1] = xb2;
+    xk1[k] = xb1;
+    xk2[k] = xb2;
+  }
+#pragma unroll 2
+  for (int i = mi - 1; i >= 0; --i) {
+    const double U1 = T(9 * i + 5), U2 = T(9 * i + 6), B1 = T(9 * i + 7), B2 = T(9 * i + 8);
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      const cxd xr = sb[k][i];
+      const cxd xk = mkc(xr.x - B1 * yb1[k].x - B2 * yb2[k].x - U1 * xk1[k].x - U2 * xk2[k].x,
+                         xr.y - B1 * yb1[k].y - B2 * yb2[k].y - U1 * xk1[k].y - U2 * xk2[k].y);
+      sb[k][i] = xk;
+      xk2[k] = xk1[k];
+      xk1[k] = xk;
+    }
+  }
+}
+
 }  // namespace hst

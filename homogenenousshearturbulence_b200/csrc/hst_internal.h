@@ -29,6 +29,7 @@ struct DeviceState {
   double2* Q;           // spectral products: [6][ncol][ny]
   double* der;          // der(0:ny-1, 0:3, -2:2)
   double* derS;         // the same, slab-major for the line-solve groups (SlabDer)
+  double* d0tab;        // the D0 matrix factored for the line-solve group (d0_factor)
   double* y;            // y(-2:ny+1)
   double* dyl;          // dyl(0:ny-1)
   double* gdamp;        // gdamp(-nz:nz, 0:nx)
@@ -74,6 +75,10 @@ cudaError_t launch_line_solve(const Geometry& g, const DeviceState& d, const Phy
 cudaError_t launch_fill_ghosts(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int field, double sx,
                                double sz, cudaStream_t st);
 size_t column_smem_bytes(const Geometry& g, int exact);
+// the factored D0 matrix of the line-solve group (P, m of g) into d.d0tab,
+// from d.derS; d0_table_doubles: the table's size for any group of ny rows
+cudaError_t launch_d0_table(const Geometry& g, const DeviceState& d, cudaStream_t st);
+size_t d0_table_doubles(int ny);
 // outstats (src/hst_stats.f90:136-285): block count of the reductions and
 // the three kernels (hst_stats.cu)
 int stats_blocks(const Geometry& g, int nsm);

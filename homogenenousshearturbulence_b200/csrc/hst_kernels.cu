@@ -34,6 +34,7 @@ struct ColumnArgs {
   const double2* Q;
   const double* der;
   const double* derS;
+  const double* d0tab;
   const double* y;
   const double* gdamp;
   int* err;   // set to 1 by a kernel whose bounded wait ran out
@@ -139,15 +140,62 @@ __global__ void k_column(ColumnArgs a) {
 
   // shift_unweighted (src/hst_equations.f90:263-293) on rhs1, rhs2, old1,
   // old2 (EXACT): D0 solve with the wrap at t, node phase, ghost rows at
-  // t+dt_sub, D0 stencil.  The scratch is this column of V1, dead here.
-  // The split stage shifts old1 and old2 first, through bufA, then loads
-  // rhs1, rhs2 (step -1), so that it holds two lines, not three.
-  const int nseq = MODE == COL_SOLVE ? (EXACT ? 5 : 1) : (EXACT ? 4 : 0);
+  // t+dt_sub, D0 stencil.  The scratch is this column of V1 (and V3), dead
+  // here.  The split stage shifts old1 and old2 as one pair of lines
+  // (through bufA, bufB and back to OLD1, OLD2), then rhs1 and rhs2, so
+  // that it holds two lines, not three; the pairs share the solves' table
+  // loads and the phases.
   const double th0 = al * sc.sx_t + be * sc.sz_t;
   double2* scr = a.V1 + (size_t)col * g.rows;
+  if (MODE == COL_SOLVE && EXACT) {
+    const double gx = al * sc.dgx + be * sc.dgz;
+    const cxd phs = cexpi(-(al * sc.sx_n + be * sc.sz_n));
+    double2* scr2 = a.V3 + (size_t)col * g.rows;
+    cxd* const bufs[2] = {bufA, bufB};
 #pragma unroll 1
-  for (int k = 0; k < nseq; ++k) {
-    const int qi = MODE == COL_SOLVE ? (EXACT ? (k < 2 ? k + 2 : (k == 2 ? -1 : k - 3)) : -1) : k;
+    for (int pass = 0; pass < 2; ++pass) {
+      const double2* s1 = pass == 0 ? a.O1 : a.R1;  // OLD1, OLD2 are written back below
+      const double2* s2 = pass == 0 ? a.O2 : a.R2;
+      for (int r = s; r < ny; r += P) {
+        bufA[G.at(r)] = s1[cb + r];
+        bufB[G.at(r)] = s2[cb + r];
+      }
+      __syncwarp(gmask);
+      group_solve_d0<P, 2>(th0, a.d0tab, G, bufs, s, gmask);
+      __syncwarp(gmask);
+      for (int r = s; r < ny; r += P) {
+        const cxd e = cexpi(-gx * a.y[r + 2]);
+        bufA[G.at(r)] = cmul(bufA[G.at(r)], e);
+        bufB[G.at(r)] = cmul(bufB[G.at(r)], e);
+      }
+      __syncwarp(gmask);
+      store_with_ghosts<P>(scr, bufA, G, ny, phs, s, false);
+      store_with_ghosts<P>(scr2, bufB, G, ny, phs, s, false);
+      __syncwarp(gmask);
+      for (int r = s; r < ny; r += P) {
+        cxd acc1 = mkc(0, 0), acc2 = mkc(0, 0);
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+          const double d0 = derv(der, ny, r, 0, j - 2);
+          const cxd v1 = scr[r + j], v2 = scr2[r + j];
+          acc1 = mkc(acc1.x + d0 * v1.x, acc1.y + d0 * v1.y);
+          acc2 = mkc(acc2.x + d0 * v2.x, acc2.y + d0 * v2.y);
+        }
+        if (pass == 0) {
+          a.O1[cb + r] = acc1;
+          a.O2[cb + r] = acc2;
+        } else {
+          bufA[G.at(r)] = acc1;
+          bufB[G.at(r)] = acc2;
+        }
+      }
+      __syncwarp(gmask);
+    }
+  }
+  const int nseq = MODE == COL_SOLVE ? 1 : (EXACT ? 4 : 0);
+#pragma unroll 1
+  for (int k = (MODE == COL_SOLVE && EXACT) ? nseq : 0; k < nseq; ++k) {
+    const int qi = MODE == COL_SOLVE ? -1 : k;
     if (qi < 0) {
       for (int r = s; r < ny; r += P) {
         bufA[G.at(r)] = a.R1[cb + r];
@@ -162,7 +210,10 @@ __global__ void k_column(ColumnArgs a) {
       for (int r = s; r < ny; r += P) X[G.at(r)] = Og[cb + r];
       __syncwarp(gmask);
     }
-    group_solve<P>(K_D0, 0.0, ni, kk, th0, DS, G, X, fac, s, gmask);
+    {
+      cxd* const bufs[1] = {X};
+      group_solve_d0<P, 1>(th0, a.d0tab, G, bufs, s, gmask);
+    }
     __syncwarp(gmask);
     for (int r = s; r < ny; r += P) {
       cxd v = cmul(X[G.at(r)], cexpi(-(al * sc.dgx + be * sc.dgz) * a.y[r + 2]));
@@ -207,7 +258,10 @@ __global__ void k_column(ColumnArgs a) {
     bufB[G.at(r)] = acc;
   }
   __syncwarp(gmask);
-  group_solve<P>(K_DY, 0.0, ni, kk, thn, DS, G, bufB, fac, s, gmask);
+  {
+    cxd* const bufs[1] = {bufB};
+    group_solve_d0<P, 1>(thn, a.d0tab, G, bufs, s, gmask);
+  }
   __syncwarp(gmask);
   // u, w from eta and dv/dy, into bufA (u) and bufB (w)
   const double rkk = c00 ? 0.0 : 1.0 / kk;
@@ -478,6 +532,7 @@ cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysSca
   a.Q = d.Q;
   a.der = d.der;
   a.derS = d.derS;
+  a.d0tab = d.d0tab;
   a.y = d.y;
   a.gdamp = d.gdamp;
   a.err = d.err;
@@ -493,6 +548,33 @@ cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysSca
     case 32: return launch_column_p<32>(a, exact, nonlin, part, st);
   }
   return cudaErrorInvalidValue;
+}
+
+// d0_factor of the group of P lanes: one warp, lanes 0..P-1
+template <int P>
+__global__ void k_d0_table(const double* __restrict__ derS, int m, double* __restrict__ tab) {
+  const int s = threadIdx.x;
+  if (s >= P) return;
+  const SlabDer DS = {derS, m, P};
+  d0_factor<P>(DS, m, s, group_mask(P), tab);
+}
+
+size_t d0_table_doubles(int ny) {
+  // d0_fields(m, P) P = 9 (ny - 2P) + P (31 + 8 levels) <= 9 ny + 32 (31 + 8 4)
+  return (size_t)9 * ny + 32 * (31 + 8 * 4);
+}
+
+cudaError_t launch_d0_table(const Geometry& g, const DeviceState& d, cudaStream_t st) {
+  if ((size_t)d0_fields(g.m, g.P) * g.P > d0_table_doubles(g.ny)) return cudaErrorInvalidValue;
+  switch (g.P) {
+    case 2: k_d0_table<2><<<1, 32, 0, st>>>(d.derS, g.m, d.d0tab); break;
+    case 4: k_d0_table<4><<<1, 32, 0, st>>>(d.derS, g.m, d.d0tab); break;
+    case 8: k_d0_table<8><<<1, 32, 0, st>>>(d.derS, g.m, d.d0tab); break;
+    case 16: k_d0_table<16><<<1, 32, 0, st>>>(d.derS, g.m, d.d0tab); break;
+    case 32: k_d0_table<32><<<1, 32, 0, st>>>(d.derS, g.m, d.d0tab); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 template <int P>
