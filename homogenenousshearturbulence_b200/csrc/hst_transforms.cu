@@ -74,9 +74,9 @@ struct TileSrc {
 };
 
 template <int NT, int PPT, typename C>
-__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256) k_zinv(Geometry g, const double2* __restrict__ V0,
-                                              const double2* __restrict__ V1, const double2* __restrict__ V2,
-                                              C* __restrict__ Z, const C* __restrict__ twz) {
+__device__ __forceinline__ void zinv_body(const Geometry& g, const double2* __restrict__ V0,
+                                          const double2* __restrict__ V1, const double2* __restrict__ V2,
+                                          C* __restrict__ Z, const C* __restrict__ twz) {
   extern __shared__ double2 sh_d[];
   C* sh = reinterpret_cast<C*>(sh_d);
   const int yt = blockIdx.x, ix = blockIdx.y, c = blockIdx.z;
@@ -85,6 +85,19 @@ __global__ void __launch_bounds__(PPT <= 8 ? 512 : 256) k_zinv(Geometry g, const
   const ZinvSrc<C> src = {V + (size_t)ix * g.nzT * g.rows + 2 + yt * Ty, g.rows, g.nz, NZ};
   const TileDst<C> dst = {Z + (((size_t)c * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
   fft_sel<NT, +1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
+}
+template <int NT, int PPT, typename C>
+__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256) k_zinv(Geometry g, const double2* __restrict__ V0,
+                                              const double2* __restrict__ V1, const double2* __restrict__ V2,
+                                              C* __restrict__ Z, const C* __restrict__ twz) {
+  zinv_body<NT, PPT, C>(g, V0, V1, V2, Z, twz);
+}
+// the FP32 1536-point plan (192 threads) held to three blocks an SM (an
+// explicit block minimum on the kernel above made the 384-point plan slower)
+__global__ void __launch_bounds__(192, 3) k_zinv_1536f(Geometry g, const double2* __restrict__ V0,
+                                                       const double2* __restrict__ V1, const double2* __restrict__ V2,
+                                                       float2* __restrict__ Z, const float2* __restrict__ twz) {
+  zinv_body<1536, 32, float2>(g, V0, V1, V2, Z, twz);
 }
 
 // --------------------------------------------------------------- k_zfwd ----
@@ -197,13 +210,14 @@ struct ProdSrc {
 #define XPROD_MINB 3
 #endif
 // launch bounds of k_xprod: 6 NX / PPT threads; the 8-point plan at 384
-// is held to 72 registers so that three 288-thread blocks fit an SM
-constexpr int xprod_threads(int NT, int PPT) { return PPT <= 8 ? (NT == 384 ? 288 : 640) : 320; }
+// is held to 72 registers so that three 288-thread blocks fit an SM, the
+// FP32 32-point plan at 1536 to two blocks
+constexpr int xprod_threads(int NT, int PPT) { return PPT <= 8 ? (NT == 384 ? 288 : 640) : (NT == 1536 ? 288 : 320); }
 #ifndef XPROD_MINB_F32
 #define XPROD_MINB_F32 4
 #endif
 constexpr int xprod_min_blocks(int NT, int PPT, int es) {
-  return PPT <= 8 && NT == 384 ? (es == 8 ? XPROD_MINB_F32 : XPROD_MINB) : 1;
+  return PPT <= 8 && NT == 384 ? (es == 8 ? XPROD_MINB_F32 : XPROD_MINB) : (NT == 1536 && es == 8 ? 2 : 1);
 }
 
 constexpr int XPROD_WAIT_LIMIT = 1 << 22;  // polls of the tile's TMA barrier before giving up
@@ -466,8 +480,13 @@ cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st
     C* Z = reinterpret_cast<C*>(d.Z);
 #define HST_ZINV(NT, PPT)                                                                                     \
   {                                                                                                           \
-    big_smem(k_zinv<NT, PPT, C>);                                                                             \
-    k_zinv<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], Z, d.twzf);      \
+    if (NT == 1536) {                                                                                         \
+      big_smem(k_zinv_1536f);                                                                                 \
+      k_zinv_1536f<<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], Z, d.twzf);          \
+    } else {                                                                                                  \
+      big_smem(k_zinv<NT, PPT, C>);                                                                           \
+      k_zinv<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], Z, d.twzf);    \
+    }                                                                                                         \
   }
     HST_FFT_DISPATCH_MP(g.nzd, g.pptz == 16, HST_ZINV);
 #undef HST_ZINV
