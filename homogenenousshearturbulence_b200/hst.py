@@ -424,7 +424,10 @@ def device_bytes(**deck) -> float:
     cfg.update(deck)
     p = Params()
     p.nx, p.ny, p.nz = int(cfg["nx"]), int(cfg["ny"]), int(cfg["nz"])
+    p.nxd, p.nzd = int(cfg.get("nxd", 0)), int(cfg.get("nzd", 0))
     p.alfa0, p.beta0, p.ly, p.re = cfg["alfa0"], cfg["beta0"], cfg["ly"], cfg["re"]
+    prec = cfg.get("precision", PREC_FP64)
+    p.precision = {"fp64": PREC_FP64, "mixed": PREC_MIXED}.get(prec, prec) if isinstance(prec, str) else int(prec)
     return float(lib().hst_gpu_device_bytes(ct.byref(p)))
 
 
