@@ -1077,6 +1077,8 @@ static int queue_timestep(hst_ctx* ctx, double* time, double deltat) {
     sc.damp_hard = (p.damp_hard && damp) ? 1 : 0;
     sc.dgx = p.S * dt_sub;
     sc.dgz = s2_integral(p, t, t + dt_sub);
+    sc.yuni = p.ystretch <= 1.0e-10 ? 1 : 0;
+    sc.ytile = p.ly * 32.0 / p.ny;
     shear_shifts(ctx, t, &sc.sx_t, &sc.sz_t);
     shear_shifts(ctx, t + dt_sub, &sc.sx_n, &sc.sz_n);
     if (ctx->column_split) {

@@ -56,6 +56,8 @@ struct SubstepScalars {
   double sx_t, sz_t;  // wrap displacements at t
   double sx_n, sz_n;  // at t + dt_sub
   int damp_hard;
+  int yuni;      // the y grid is uniform (ystretch 0): y(r + 32) - y(r) = ytile
+  double ytile;  // 32 ly / ny
 };
 
 struct PhysScalars {
