@@ -153,11 +153,17 @@ struct hst_ctx {
   double prof_ms[HST_KC_N];
   long long prof_n[HST_KC_N];
   // asynchronous host I/O of V1..V3 (hst_gpu_upload_async and friends): a
-  // copy-in and a copy-out stream, and a device snapshot of each component
-  // that the copy-out stream reads while the solver goes on
+  // copy-in and a copy-out stream; per component a device staging copy that
+  // the copy-in stream fills while the solver still works on the previous
+  // contents, and a device snapshot that the copy-out stream reads while the
+  // solver goes on, each with the event that frees it again
   cudaStream_t s_in = nullptr, s_out = nullptr;
   cudaEvent_t ev_main = nullptr, ev_in = nullptr, ev_stage = nullptr, ev_out = nullptr;
   double2* snap[3] = {nullptr, nullptr, nullptr};
+  double2* stage[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_staged[3] = {nullptr, nullptr, nullptr};  // stage[c] copied into V (solver's stream)
+  cudaEvent_t ev_read[3] = {nullptr, nullptr, nullptr};    // snap[c] copied to the host (copy-out stream)
+  bool staged_used[3] = {false, false, false}, read_used[3] = {false, false, false};
 };
 
 // Runs `launch` (which queues one kernel on ctx->stream) between two events
@@ -575,7 +581,13 @@ extern "C" int hst_gpu_destroy(hst_ctx* ctx) {
     }
   for (cudaEvent_t e : {ctx->ev_main, ctx->ev_in, ctx->ev_stage, ctx->ev_out})
     if (e) cudaEventDestroy(e);
+  for (int c = 0; c < 3; ++c) {
+    if (ctx->ev_staged[c]) cudaEventDestroy(ctx->ev_staged[c]);
+    if (ctx->ev_read[c]) cudaEventDestroy(ctx->ev_read[c]);
+  }
   for (double2* q : ctx->snap)
+    if (q) cudaFree(q);
+  for (double2* q : ctx->stage)
     if (q) cudaFree(q);
   for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
   free_device(ctx);
@@ -645,6 +657,10 @@ static int ensure_io(hst_ctx* ctx) {
   CK(cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking));
   for (cudaEvent_t* e : {&ctx->ev_main, &ctx->ev_in, &ctx->ev_stage, &ctx->ev_out})
     CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  for (int c = 0; c < 3; ++c) {
+    CK(cudaEventCreateWithFlags(&ctx->ev_staged[c], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ctx->ev_read[c], cudaEventDisableTiming));
+  }
   return HST_OK;
 }
 
@@ -653,13 +669,24 @@ extern "C" int hst_gpu_upload_async(hst_ctx* ctx, int field, const double* host)
   CK(cudaSetDevice(ctx->device));
   int rc = ensure_io(ctx);
   if (rc != HST_OK) return rc;
-  // after everything queued so far on the solver's stream (the snapshot
-  // copies of earlier downloads included), before anything queued later
-  CK(cudaEventRecord(ctx->ev_main, ctx->stream));
-  CK(cudaStreamWaitEvent(ctx->s_in, ctx->ev_main, 0));
-  CK(cudaMemcpyAsync(ctx->d.F[field], host, sizeof(double2) * ctx->g.nf, cudaMemcpyHostToDevice, ctx->s_in));
+  const size_t bytes = sizeof(double2) * ctx->g.nf;
+  if (!ctx->stage[field] && cudaMalloc((void**)&ctx->stage[field], bytes) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->stage[field] = nullptr;
+    return fail(ctx, HST_ENOMEM, "upload_async: staging copy of %.2f GB refused", bytes / 1e9);
+  }
+  // host -> staging copy on the copy-in stream, as soon as the solver's
+  // stream has moved the previous upload of this component into V (so it
+  // runs beside the work queued before this call); then staging -> V on
+  // the solver's stream, after everything queued so far, before anything
+  // queued later
+  if (ctx->staged_used[field]) CK(cudaStreamWaitEvent(ctx->s_in, ctx->ev_staged[field], 0));
+  CK(cudaMemcpyAsync(ctx->stage[field], host, bytes, cudaMemcpyHostToDevice, ctx->s_in));
   CK(cudaEventRecord(ctx->ev_in, ctx->s_in));
   CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_in, 0));
+  CK(cudaMemcpyAsync(ctx->d.F[field], ctx->stage[field], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaEventRecord(ctx->ev_staged[field], ctx->stream));
+  ctx->staged_used[field] = true;
   return HST_OK;
 }
 
@@ -674,13 +701,15 @@ extern "C" int hst_gpu_download_async(hst_ctx* ctx, int field, double* host) {
     ctx->snap[field] = nullptr;
     return fail(ctx, HST_ENOMEM, "download_async: snapshot of %.2f GB refused", bytes / 1e9);
   }
-  // the snapshot may be overwritten once the previous copy-out has read it
-  CK(cudaEventRecord(ctx->ev_out, ctx->s_out));
-  CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_out, 0));
+  // the snapshot may be overwritten once the previous copy-out of this
+  // component has read it
+  if (ctx->read_used[field]) CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_read[field], 0));
   CK(cudaMemcpyAsync(ctx->snap[field], ctx->d.F[field], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
   CK(cudaEventRecord(ctx->ev_stage, ctx->stream));
   CK(cudaStreamWaitEvent(ctx->s_out, ctx->ev_stage, 0));
   CK(cudaMemcpyAsync(host, ctx->snap[field], bytes, cudaMemcpyDeviceToHost, ctx->s_out));
+  CK(cudaEventRecord(ctx->ev_read[field], ctx->s_out));
+  ctx->read_used[field] = true;
   return HST_OK;
 }
 

@@ -117,9 +117,13 @@ int hst_gpu_download(hst_ctx* ctx, int field, double* host);
  * with the solver.  No counterpart in the reference, whose target updates
  * (src/hst.f90:76,110,121,141) are synchronous.
  *   upload_async:   the host buffer (pinned: cudaHostAlloc / registered)
- *                   is copied in on a copy-in stream after all work queued
- *                   so far; work queued later waits for it.  The buffer must
- *                   not change until hst_gpu_wait_io.
+ *                   is copied on a copy-in stream into a device staging
+ *                   copy of the component (which may overlap the work
+ *                   queued so far), and from there into the field on the
+ *                   solver's stream after all work queued so far; work
+ *                   queued later sees the new field.  The buffer must not
+ *                   change until hst_gpu_wait_io.  The first call per
+ *                   component allocates its staging copy.
  *   download_async: the field as it is at this point of the queue (a
  *                   device snapshot, taken on the solver's stream) is copied
  *                   out on a copy-out stream; the host buffer is valid after
