@@ -165,10 +165,15 @@ __global__ void k_column(ColumnArgs a) {
       __syncwarp(gmask);
       group_solve_d0<P, 2>(th0, a.d0tab, G, bufs, s, gmask);
       __syncwarp(gmask);
+      // the node phase exp(-i gx y(r)); on a uniform grid by one product a
+      // row from the lane's first row (rows s, s + P, ... are P dy apart)
+      cxd e = cexpi(-gx * a.y[s + 2]);
+      const cxd estep = sc.yuni ? cexpi(-gx * (sc.ytile * (P / 32.0))) : mkc(1.0, 0.0);
       for (int r = s; r < ny; r += P) {
-        const cxd e = cexpi(-gx * a.y[r + 2]);
+        if (!sc.yuni && r != s) e = cexpi(-gx * a.y[r + 2]);
         bufA[G.at(r)] = cmul(bufA[G.at(r)], e);
         bufB[G.at(r)] = cmul(bufB[G.at(r)], e);
+        e = cmul(e, estep);
       }
       __syncwarp(gmask);
       store_with_ghosts<P>(scr, bufA, G, ny, phs, s, false);
