@@ -1,16 +1,20 @@
 #!/usr/bin/env python
 """Benchmark of the hst RK3 / Crank-Nicolson substep on B200s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c3]
 
 One step is one RK3 time step (three substeps, hst_gpu_timestep, with the
 CFL read-back the Fortran time loop does every step); the metric is
-substeps per second of the whole job.  Default workload:
-the plain FP64 drop-in at 384x384 dealiased x 256 (deck nx = 127, nz = 128,
-ny = 256; ly = 2 pi, alfa0 = beta0 = 1, S = 1, Re = 2000, dt = 0.002) from a
-seeded divergence-free field with E(k) ~ k^4 exp(-2 (k/8)^2), energy 0.1.
-The fields (0.4 GB per set of three components) are larger than L2, so no
-flush is needed between steps.
+substeps per second of the whole job.  Default workload: the plain FP64
+drop-in at 768x768 dealiased x 512 ("512^3": deck nx = 255, nz = 256,
+ny = 512; ly = 2 pi, alfa0 = beta0 = 1, S = 1, Re = 5000, dt = 0.001,
+exact_shift) from a seeded divergence-free field with
+E(k) ~ k^4 exp(-2 (k/16)^2), energy 0.1.  The same line carries the
+mixed-precision form on the same field (`mixed`), each form's error against
+the oracle after the same substeps (`accuracy`), the end-to-end rate through
+the C ABI with host buffers (`e2e`), the roofline of the top kernel and of
+the whole substep, and the oracle timed on the host cores (`cpu_baseline`).
+The fields (gigabytes) are far larger than L2, so no flush is needed.
 
 N > 1 (one process per GPU under torch.distributed.run): independent
 replicas of the single-field path, which does not shard (the reference's
@@ -20,7 +24,9 @@ the max over ranks of the device-timed region.
 
 --impl reference: the reference's CPU path on the host cores.  The
 reference (Fortran + MPI + FFTW) cannot be built in this image, so its
-restatement in oracle/ is timed instead (all host threads), rank 0 only.
+restatement in oracle/ is timed instead (all host threads), rank 0 only;
+each of its steps is one substep of the same workload (a bounded sample:
+a substep of the 768^2 x 512 field takes the host seconds).
 """
 from __future__ import annotations
 
@@ -41,27 +47,15 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 PI = math.pi
-CONFIGS = {
-    # 96^2 x 64, Re 1000, dt 0.005, k0 4
-    "c1": dict(deck=dict(nx=31, ny=64, nz=32, alfa0=1.0, beta0=1.0, ly=2 * PI, re=1000.0, S=1.0, deltat=0.005),
-               k0=4.0, label="FP64 substep, 96x96 dealiased x 64 (nx=31, nz=32, ny=64), Re 1000, dt 0.005"),
-    # 384^2 x 256, Re 2000, dt 0.002, k0 8
-    "c2": dict(deck=dict(nx=127, ny=256, nz=128, alfa0=1.0, beta0=1.0, ly=2 * PI, re=2000.0, S=1.0, deltat=0.002),
-               k0=8.0, label="FP64 substep, 384x384 dealiased x 256 (nx=127, nz=128, ny=256), Re 2000, dt 0.002"),
-    # 768^2 x 512 in FP64, Re 5000, dt 0.001, exact_shift, k0 16
-    "c3": dict(deck=dict(nx=255, ny=512, nz=256, alfa0=1.0, beta0=1.0, ly=2 * PI, re=5000.0, S=1.0, deltat=0.001,
-                         exact_shift=True),
-               k0=16.0, label="FP64 substep, 768x768 dealiased x 512 (nx=255, nz=256, ny=512), exact_shift"),
-    # 1536^2 x 512, Re 10000, dt 0.0005, exact_shift, S2(t) = 0.5 sin(2 pi t / 10), the hard large-scale damping
-    # mask with semi-axes 2 (following the shear angle), k0 24; meant for --precision mixed (72 GB; FP64 114 GB).
-    # No CPU baseline: one oracle time step of this size needs over 100 GB of host memory and minutes.
-    "c5": dict(deck=dict(nx=511, ny=512, nz=512, alfa0=1.0, beta0=1.0, ly=2 * PI, re=10000.0, S=1.0, deltat=0.0005,
-                         exact_shift=True, s2_amplitude=0.5, s2_period=10.0, damp_kpar=2.0, damp_kperp=2.0,
-                         damp_hard=True),
-               k0=24.0, cpu_baseline=False,
-               label="FP64 substep, 1536x1536 dealiased x 512 (nx=511, nz=512, ny=512), Re 10000, dt 0.0005, "
-                     "exact_shift, S2 = 0.5 sin(2 pi t/10), hard damping inside |k| < 2"),
-}
+
+from homogenenousshearturbulence_b200.workloads import ENSEMBLE, ENSEMBLE_COMMON, ENSEMBLE_K0, WORKLOADS  # noqa: E402
+
+# the workloads this script times, with the substeps of the oracle run that
+# gives the CPU baseline and the accuracy (about 10-30 s of host time on 16
+# threads; one warm-up substep first); the 1536^2 x 512 field has no CPU leg:
+# one oracle substep of it needs about 90 GB of host memory and minutes
+CONFIGS = {k: dict(v, label="FP64 substep, " + v["label"]) for k, v in WORKLOADS.items()}
+ORACLE_SUBSTEPS = {"c1": 60, "c2": 12, "c3": 3, "c5": 0}
 
 
 def peaks():
@@ -156,14 +150,6 @@ def seeded_field(cfg, y):
                             energy=0.1)
 
 
-# The ensemble of independent realisations with uneven sizes: 24 members of
-# 192^2 x 128 (deck nx = 63, nz = 64, ny = 128) and 8 of 384^2 x 192 (nx = 95,
-# nz = 96, ny = 192; the reference pads nxd, nzd to 192, 384), seeds 1..32,
-# Re 1500, dt 0.004, k0 6, energy 0.1.
-ENSEMBLE = [dict(nx=63, ny=128, nz=64)] * 24 + [dict(nx=95, ny=192, nz=96)] * 8
-ENSEMBLE_COMMON = dict(alfa0=1.0, beta0=1.0, ly=2 * PI, re=1500.0, S=1.0, deltat=0.004)
-
-
 def run_ensemble(args, dev):
     """Every member in its own context and stream: the concurrent form queues
     one time step of each member in turn (hst_gpu_timesteps, no host wait)
@@ -179,7 +165,7 @@ def run_ensemble(args, dev):
         deck = dict(ENSEMBLE_COMMON, **sz, precision=args.precision)
         s = hst.Solver(deck, device=dev)
         V0 = hst.random_field(deck["nx"], deck["ny"], deck["nz"], deck["alfa0"], deck["beta0"], deck["ly"], s.y,
-                              seed=i + 1, k0=6.0, energy=0.1)
+                              seed=i + 1, k0=ENSEMBLE_K0, energy=0.1)
         s.time = 0.0
         s.set_velocity(V0)
         members.append(s)
@@ -249,33 +235,54 @@ def whole_job_rate(world, units_per_rank, ms_max):
     return world * units_per_rank / (ms_max / 1000.0)
 
 
-def cpu_oracle_rate(cfg, steps, budget_s=60.0, warmup=1):
+def oracle_substeps(cfg, warmup, timed, V0=None):
     """The oracle (the reference's CPU path restated, all host threads) on
-    the same workload; returns (substeps/s, steps timed, threads, warm-up
-    steps)."""
+    the workload from its seeded field: `warmup` untimed substeps, then
+    `timed` timed ones (substep i of a time step is i mod 3).  Returns
+    (substeps/s, threads, the velocity after all of them, the time)."""
     import oracle
-    from tests.gpu_util import deck_to_oracle
     d = dict(cfg["deck"])
-    o = oracle.Sim(deck_to_oracle(d))
+    o = oracle.Sim(oracle.params_from_deck(d))
+    if V0 is None:
+        V0 = seeded_field(cfg, o.y())
+    for c in range(3):
+        o.field(c)[...] = V0[c]
+        o.fill_ghosts(c)
+    o.time = 0.0
+    o.deltat = d["deltat"]
+    for k in range(warmup):
+        o.substep(k % 3)
+    t0 = time.perf_counter()
+    for k in range(warmup, warmup + timed):
+        o.substep(k % 3)
+    el = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    V = np.stack([o.field(c).copy() for c in range(3)])
+    return (timed / el if timed else float("nan")), threads, V, o.time
+
+
+def cpu_oracle_rate(cfg, steps, budget_s=60.0, warmup=1):
+    """Substeps/s of the oracle on the workload: one warm-up substep, then
+    timed substeps within the budget (at most 3 steps); returns (substeps/s,
+    substeps timed, threads, warm-up substeps)."""
+    import oracle
+    d = dict(cfg["deck"])
+    o = oracle.Sim(oracle.params_from_deck(d))
     V0 = seeded_field(cfg, o.y())
     for c in range(3):
         o.field(c)[...] = V0[c]
         o.fill_ghosts(c)
     o.deltat = d["deltat"]
     t0 = time.perf_counter()
-    o.timestep()  # warm-up step (page-in, plans)
+    o.substep(0)
     first = time.perf_counter() - t0
-    # the rest of the warm-up and the timed steps within the budget
-    w = max(0, min(warmup - 1, int(0.25 * budget_s / max(first, 1e-6))))
-    for _ in range(w):
-        o.timestep()
-    n = max(1, min(steps, int(budget_s / max(first, 1e-6))))
+    n = max(1, min(3 * steps, int(budget_s / max(first, 1e-6))))
     t0 = time.perf_counter()
-    for _ in range(n):
-        o.timestep()
+    for k in range(1, 1 + n):
+        o.substep(k % 3)
     el = time.perf_counter() - t0
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return 3 * n / el, n, threads, 1 + w
+    return n / el, n, threads, 1
 
 
 def ensemble_main(args):
@@ -291,21 +298,21 @@ def ensemble_main(args):
     if args.impl == "reference":
         if rank != 0:
             return 0
-        cfg = dict(deck=dict(ENSEMBLE_COMMON, **ENSEMBLE[0]), k0=6.0)
+        cfg = dict(deck=dict(ENSEMBLE_COMMON, **ENSEMBLE[0]), k0=ENSEMBLE_K0)
         rate, n, threads, w = cpu_oracle_rate(cfg, args.steps, budget_s=60.0, warmup=args.warmup)
         # the members one after another: a substep of every member takes
         # 24 small and 8 large member-substeps
         small = rate
-        big_cfg = dict(deck=dict(ENSEMBLE_COMMON, **ENSEMBLE[-1]), k0=6.0)
+        big_cfg = dict(deck=dict(ENSEMBLE_COMMON, **ENSEMBLE[-1]), k0=ENSEMBLE_K0)
         rate_b, nb, _, _ = cpu_oracle_rate(big_cfg, 1, budget_s=30.0, warmup=1)
         per_step = 24 / small + 8 / rate_b  # seconds per substep of every member
         agg = 32 / per_step
         line = {"metric": "substeps_per_s", "value": agg, "unit": unit, "impl": "reference", "n_gpus": args.gpus,
-                "steps": n, "warmup": w, "ms_per_step": 3000.0 * 32 / agg, "higher_is_better": True,
+                "steps": n, "warmup": w, "ms_per_step": 1000.0 * 32 / agg, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": label, "members": 32},
                 "cpu_baseline": {"value": agg, "unit": unit, "cores": threads, "kind": "port",
-                                 "sample": f"{n} + {nb} time steps of a small and a large member (oracle, all host "
+                                 "sample": f"{n} + {nb} substeps of a small and a large member (oracle, all host "
                                            f"threads), the members taken one after another"},
                 "e2e": {"value": agg, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -338,40 +345,109 @@ def ensemble_main(args):
     return 0
 
 
+def time_steps(s, dt, steps, stream, barrier, clocks=None):
+    """`steps` time steps of context s between two CUDA events on its stream,
+    with a barrier and a device synchronisation on both sides; returns the
+    milliseconds, the per-kernel device times and the kernel launches."""
+    import torch
+    barrier()
+    launches0 = s.launches
+    s.reset_kernel_times()
+    s.set_profiling(True)
+    if clocks is not None:
+        clocks.start()
+        time.sleep(0.3)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        s.timestep(dt)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop() if clocks is not None else None
+    s.set_profiling(False)
+    kt = {k: v for k, v in s.kernel_times().items() if v[1] > 0}
+    if not math.isfinite(s.cfl):
+        raise SystemExit("non-finite CFL: the run blew up")
+    return ms, kt, s.launches - launches0, clk
+
+
+def roofline(deck, s, kt, mixed, sub_ms, config):
+    """The top kernel's roofline (its algorithmic bytes per launch over its
+    average launch time, against the measured HBM copy bandwidth) and the
+    whole substep's (B_alg over the substep time)."""
+    per_kernel, b_sub, Ns, Nzx = alg_bytes(deck, s.nxd, s.nzd, kt.get("rhs", (0, 0))[1] > 0, mixed)
+    peak, peak_kind = peaks()
+    top = max(kt, key=lambda k: kt[k][0])
+    avg_ms = kt[top][0] / kt[top][1]
+    achieved = per_kernel[top] / (avg_ms / 1000.0) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / f"traffic_{config}{'_mixed' if mixed else ''}.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(top)
+    roof = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_kind": peak_kind, "traffic": traffic, "alg_bytes_per_launch": per_kernel[top],
+            "avg_launch_ms": avg_ms}
+    sub = {"alg_bytes": b_sub, "ms_per_substep": sub_ms, "achieved_gbs": b_sub / (sub_ms / 1000.0) / 1e9,
+           "frac": b_sub / (sub_ms / 1000.0) / 1e9 / peak}
+    return roof, sub, {k: v[0] / v[1] for k, v in kt.items()}, {k: v[0] / sum(x[0] for x in kt.values())
+                                                                for k, v in kt.items()}
+
+
+def reference_main(args, cfg):
+    """--impl reference: the oracle port of the reference's CPU path on all
+    host threads, rank 0 only; each step is one substep of the workload from
+    its seeded field (W warm-up substeps, then K timed)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    unit = "substeps/s"
+    if not cfg.get("cpu_baseline", True):
+        print(json.dumps({"impl": "reference", "unavailable": "one oracle substep of this workload needs more host "
+                                                              "memory than the box is assumed to have"}), flush=True)
+        return 0
+    rate, threads, _, _ = oracle_substeps(cfg, args.warmup, args.steps)
+    line = {"metric": "substeps_per_s", "value": rate, "unit": unit, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / rate, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["label"], "step": "one substep of the workload (a bounded sample; the "
+                                                         "GPU arm's steps are whole RK3 time steps of 3 substeps)"},
+            "cpu_baseline": {"value": rate, "unit": unit, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} substeps of the workload from its seeded field after "
+                                       f"{args.warmup} warm-up substeps (the oracle restatement of the reference "
+                                       f"CPU path on {threads} threads; the Fortran+MPI+FFTW build is not "
+                                       f"buildable in this image)"},
+            "e2e": {"value": rate, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS) + ["c4"])
+    ap.add_argument("--config", default="c3", choices=sorted(CONFIGS) + ["c4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="precision of the ensemble members (--config c4)")
     args = ap.parse_args()
     if args.config == "c4":
         return ensemble_main(args)
     cfg = CONFIGS[args.config]
+    cfg = dict(cfg, cpu_baseline=ORACLE_SUBSTEPS[args.config] > 0)
+    if args.impl == "reference":
+        return reference_main(args, cfg)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     metric, unit = "substeps_per_s", "substeps/s"
-
-    if args.impl == "reference":
-        if rank != 0:
-            return 0
-        rate, n, threads, w = cpu_oracle_rate(cfg, args.steps, budget_s=90.0, warmup=args.warmup)
-        line = {"metric": metric, "value": rate, "unit": unit, "impl": "reference", "n_gpus": args.gpus,
-                "steps": n, "warmup": w, "ms_per_step": 3000.0 / rate, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": cfg["label"], "step": "one RK3 time step = 3 substeps"},
-                "cpu_baseline": {"value": rate, "unit": unit, "cores": threads, "kind": "port",
-                                 "sample": f"{n} time steps of the same workload after {w} warm-up step(s) (the oracle "
-                                           f"restatement of the reference CPU path; the Fortran+MPI+FFTW build is not "
-                                           f"buildable in this image)"},
-                "e2e": {"value": rate, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return 0
 
     import torch
     from homogenenousshearturbulence_b200 import hst
@@ -385,72 +461,35 @@ def main():
     torch.cuda.set_device(dev)
     deck = dict(cfg["deck"])
     dt = deck["deltat"]
-    mixed = args.precision == "mixed"
-    accuracy = None
-    V0 = vb = None
-    if mixed:
-        # the error of the mixed-precision form against the FP64 form after
-        # 30 substeps from the same field, on this GPU (the FP64 context
-        # first and alone: both at 1536^2 x 512 would not fit)
-        ref = hst.Solver(deck, device=dev)
-        V0 = seeded_field(cfg, ref.y)
-        ref.time = 0.0
-        ref.set_velocity(V0)
-        ref.timesteps(10, dt)
-        vb = ref.velocity()
-        ref.close()
-    s = hst.Solver(dict(deck, precision=args.precision), device=dev)
-    if V0 is None:
-        V0 = seeded_field(cfg, s.y)
-    if mixed:
+    n_acc = ORACLE_SUBSTEPS[args.config] if (world == 1 and not args.no_cpu_baseline) else 0
+    gpu_acc = {}
+
+    def barrier_of(s):
+        def barrier():
+            torch.cuda.synchronize(dev)
+            s.sync()
+            if dist is not None:
+                dist.barrier()
+        return barrier
+
+    # ---- the FP64 drop-in (the headline)
+    s = hst.Solver(deck, device=dev)
+    V0 = seeded_field(cfg, s.y)
+    stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", dev))
+    barrier = barrier_of(s)
+    if n_acc:
         s.time = 0.0
         s.set_velocity(V0)
-        s.timesteps(10, dt)
-        num = den = 0.0
-        for c in range(3):
-            va = s.download(c)
-            num += float(np.linalg.norm((va - vb[c])[..., 2:-2]) ** 2)
-            den += float(np.linalg.norm(vb[c][..., 2:-2]) ** 2)
-        accuracy = {"rel_l2_vs_fp64": math.sqrt(num / den), "substeps": 30}
-        del vb, va
+        s.timesteps(n_acc // 3, dt)
+        gpu_acc["fp64"] = s.velocity()
     s.time = 0.0
     s.set_velocity(V0)
-    stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", dev))
-
-    def barrier():
-        torch.cuda.synchronize(dev)
-        s.sync()
-        if dist is not None:
-            dist.barrier()
-
     for _ in range(args.warmup):
         s.timestep(dt)
-    barrier()
-    launches0 = s.launches
-    s.reset_kernel_times()
-    s.set_profiling(True)
-    clocks = ClockSampler(dev)
-    clocks.start()
-    time.sleep(0.3)
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        s.timestep(dt)
-    e1.record(stream)
-    e1.synchronize()
-    barrier()
-    ms = e0.elapsed_time(e1)
-    clk = clocks.stop()
-    s.set_profiling(False)
-    ktimes = s.kernel_times()
-    launches = s.launches - launches0
+    ms, kt, launches, clk = time_steps(s, dt, args.steps, stream, barrier, ClockSampler(dev))
     ms = reduce_max(ms, dist, f"cuda:{dev}")
     nsub = 3 * args.steps
     value = whole_job_rate(world, nsub, ms)
-    if not math.isfinite(s.cfl):
-        raise SystemExit("non-finite CFL: the run blew up")
 
     # end to end through the public API with host buffers: every step
     # uploads the three velocity components from pinned memory, advances
@@ -493,58 +532,80 @@ def main():
         mse = reduce_max(mse, dist, f"cuda:{dev}")
         e2e = {"value": whole_job_rate(world, 3 * ke, mse), "unit": unit, "h2d_bytes_per_step": 3 * nbytes,
                "d2h_bytes_per_step": 3 * nbytes, "steps": ke}
+        del pin_in, pin_out
+    roof, sub_roof, kms, kshare = roofline(deck, s, kt, False, ms / nsub, args.config)
+    nxd, nzd = s.nxd, s.nzd
+    s.close()
+
+    # ---- the mixed-precision form on the same field
+    mixed = None
+    if not args.no_mixed:
+        m = hst.Solver(dict(deck, precision="mixed"), device=dev)
+        mstream = torch.cuda.ExternalStream(m.stream, device=torch.device("cuda", dev))
+        if n_acc:
+            m.time = 0.0
+            m.set_velocity(V0)
+            m.timesteps(n_acc // 3, dt)
+            gpu_acc["mixed"] = m.velocity()
+        m.time = 0.0
+        m.set_velocity(V0)
+        for _ in range(args.warmup):
+            m.timestep(dt)
+        mms, mkt, mlaunches, _ = time_steps(m, dt, args.steps, mstream, barrier_of(m))
+        mms = reduce_max(mms, dist, f"cuda:{dev}")
+        mroof, msub, mkms, _ = roofline(deck, m, mkt, True, mms / nsub, args.config)
+        mixed = {"value": whole_job_rate(world, nsub, mms), "unit": unit, "ms_per_step": mms / args.steps,
+                 "speedup_vs_fp64": ms / mms, "dtype": "f32+f64",
+                 "form": "FP32 x-z transforms, products and product spectra; FP64 right-hand sides, shift, solves "
+                         "and u, w",
+                 "roofline": mroof, "substep_roofline": msub, "kernels_ms_per_launch": mkms,
+                 "gpu_launches": mlaunches}
+        m.close()
 
     if rank == 0:
-        per_kernel, b_sub, Ns, Nzx = alg_bytes(deck, s.nxd, s.nzd, ktimes.get("rhs", (0, 0))[1] > 0, mixed)
-        peak, peak_kind = peaks()
-        kt = {k: v for k, v in ktimes.items() if v[1] > 0}
-        top = max(kt, key=lambda k: kt[k][0])
-        avg_ms = kt[top][0] / kt[top][1]
-        achieved = per_kernel[top] / (avg_ms / 1000.0) / 1e9
-        traffic = None
-        tf = ROOT / "profiles" / f"traffic_{args.config}.json"
-        if tf.exists() and not mixed:
-            traffic = json.loads(tf.read_text()).get(top)
-        sub_ms = ms / nsub
         line = {
             "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
-            "config": {"workload": (cfg["label"].replace("FP64 substep", "substep")
-                                    + ", mixed precision (FP32 transforms, products and spectra; FP64 right-hand "
-                                      "sides, shift and solves)") if mixed else cfg["label"],
-                       "precision": args.precision,
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["label"], "precision": "fp64",
                        "step": "one RK3 time step = 3 substeps (hst_gpu_timestep)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single field, 1 GPU",
-                       "l2": "inputs larger than L2 (no flush)", "nxd": s.nxd, "nzd": s.nzd,
-                       },
-            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                         "alg_bytes_per_launch": per_kernel[top], "avg_launch_ms": avg_ms},
-            "substep_roofline": {"alg_bytes": b_sub, "ms_per_substep": sub_ms,
-                                 "achieved_gbs": b_sub / (sub_ms / 1000.0) / 1e9,
-                                 "frac": b_sub / (sub_ms / 1000.0) / 1e9 / peak},
-            "kernels_ms_per_launch": {k: v[0] / v[1] for k, v in kt.items()},
-            "kernel_share": {k: v[0] / sum(x[0] for x in kt.values()) for k, v in kt.items()},
+                       "l2": "inputs larger than L2 (no flush)", "nxd": nxd, "nzd": nzd},
+            "roofline": roof, "substep_roofline": sub_roof,
+            "kernels_ms_per_launch": kms, "kernel_share": kshare,
             "gpu_launches": launches,
             "clocks": clk,
         }
         if e2e:
             line["e2e"] = e2e
-        if accuracy:
-            line["accuracy"] = accuracy
-        if world == 1 and not args.no_cpu_baseline and cfg.get("cpu_baseline", True):
-            rate, n, threads, w = cpu_oracle_rate(cfg, 2, budget_s=20.0)
+        if mixed:
+            line["mixed"] = mixed
+        if n_acc:
+            # the oracle from the same seeded field: one warm-up substep, the
+            # rest timed (the CPU baseline), its final velocity the reference
+            # of both forms' accuracy after the same substeps
+            rate, threads, Vo, _ = oracle_substeps(cfg, 1, n_acc - 1, V0)
             line["cpu_baseline"] = {"value": rate, "unit": unit, "cores": threads, "kind": "port",
-                                    "sample": f"{n} time step(s) of the same workload after {w} warm-up step, oracle "
-                                              f"restatement of the reference CPU path, {threads} threads"}
+                                    "sample": f"{n_acc - 1} substeps of the same workload from its seeded field "
+                                              f"after 1 warm-up substep, oracle restatement of the reference CPU "
+                                              f"path, {threads} threads"}
+
+            def rel_l2(a, b):
+                a, b = a[..., 2:-2], b[..., 2:-2]
+                return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+            acc = {"substeps": n_acc, "against": "the oracle (FP64 CPU restatement of the reference path) from "
+                                                 "the same seeded field, relative L2 over the interior rows"}
+            for k, Vg in gpu_acc.items():
+                acc[f"{k}_rel_l2_vs_oracle"] = rel_l2(Vg, Vo)
+            line["accuracy"] = acc
+            if mixed and "mixed" in gpu_acc:
+                mixed["rel_l2_vs_oracle"] = acc["mixed_rel_l2_vs_oracle"]
         print(json.dumps(line), flush=True)
-    s.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     return 0
-
 
 if __name__ == "__main__":
     sys.exit(main())

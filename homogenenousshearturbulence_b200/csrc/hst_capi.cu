@@ -12,6 +12,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 #include "hst_dev.cuh"
@@ -141,6 +142,7 @@ struct hst_ctx {
   double* h_gdamp;                // pinned staging of gdamp uploads
   unsigned long long* h_cfl;      // pinned CFL read-back
   std::string err;
+  std::unordered_set<const void*> configured;  // kernels whose shared-memory limit is raised
   long long launches;
   int device;
   // the column stage as two kernels (right-hand sides streamed row by row,
@@ -408,6 +410,7 @@ static void free_device(hst_ctx* c) {
   for (void* q : ps)
     if (q) cudaFree(q);
   std::memset(&d, 0, sizeof d);
+  d.configured = &c->configured;
 }
 
 extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
@@ -430,6 +433,7 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   ctx->h_gdamp = nullptr;
   ctx->h_cfl = nullptr;
   std::memset(&ctx->d, 0, sizeof ctx->d);
+  ctx->d.configured = &ctx->configured;
   std::string why;
   int rc = choose_geometry(*pin, ctx->g, why);
   if (rc != HST_OK) {
@@ -452,7 +456,7 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   const hst_gpu_params& p = ctx->p;
   const Geometry& g = ctx->g;
   ctx->device = p.device;
-  // derived quantities (src/hst_input.f90:206-215)
+  // derived quantities (src/hst_input.f90:92-102)
   ctx->lx = 2.0 * PI / p.alfa0;
   ctx->lz = 2.0 * PI / p.beta0;
   ctx->ps.alfa0 = p.alfa0;

@@ -21,6 +21,12 @@ __device__ __forceinline__ cxd cmuli(double b, cxd a) { return mkc(-b * a.y, b *
 // a - s * b (s real)
 __device__ __forceinline__ cxd cfms(cxd a, double s, cxd b) { return mkc(a.x - s * b.x, a.y - s * b.y); }
 __device__ __forceinline__ cxd cdivr(cxd a, double d) { return mkc(a.x / d, a.y / d); }
+// max that propagates NaN (fmax returns the other operand), as a positive
+// quiet NaN
+__device__ __forceinline__ double nan_max(double a, double b) {
+  if (a != a || b != b) return __longlong_as_double(0x7ff8000000000000LL);
+  return fmax(a, b);
+}
 __device__ __forceinline__ cxd cexpi(double x) {
   double s, c;
   sincos(x, &s, &c);

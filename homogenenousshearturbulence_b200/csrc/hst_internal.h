@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <unordered_set>
+
 #include "../../include/hst_gpu.h"
 
 namespace hst {
@@ -46,7 +48,22 @@ struct DeviceState {
   int nsm;        // SMs of the device
   double* stats;  // outstats scratch: block partials of the moments (9 a block), of the three
                   // gradients (one a block each), then the 8 results
+  // kernels whose shared-memory limit has been raised in this context
+  // (owned by the context; null: raise it at every launch)
+  std::unordered_set<const void*>* configured;
 };
+
+// Raises kernel k's dynamic shared-memory limit to `bytes`, once per context
+// (the attribute belongs to the function in the current context; setting it
+// at every launch costs a driver call each time).
+template <typename K>
+inline cudaError_t smem_limit(const DeviceState& d, K k, int bytes) {
+  const void* key = reinterpret_cast<const void*>(k);
+  if (d.configured && d.configured->count(key)) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && d.configured) d.configured->insert(key);
+  return e;
+}
 
 // Scalars of one substep of the column kernel.
 struct SubstepScalars {

@@ -39,6 +39,7 @@ struct ColumnArgs {
   const double* gdamp;
   int* err;   // set to 1 by a kernel whose bounded wait ran out
   int tiled;  // the right-hand sides through k_rhs_tiled
+  const DeviceState* dstate;  // host side only: the launch's context state
 };
 
 __device__ __forceinline__ unsigned group_mask(int P) {
@@ -496,12 +497,10 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
     const size_t smem = (size_t)RT_WARPS * 2 * RT_STAGE * sizeof(double2);
     const int blocks = (g.ncol + RT_WARPS - 1) / RT_WARPS;
     if (g.mp) {
-      cudaFuncSetAttribute(k_rhs_tiled<EXACT, NONLIN, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+      smem_limit(*a.dstate, k_rhs_tiled<EXACT, NONLIN, float2>, (int)smem);
       k_rhs_tiled<EXACT, NONLIN, float2><<<blocks, 32 * RT_WARPS, smem, st>>>(a, a.err);
     } else {
-      cudaFuncSetAttribute(k_rhs_tiled<EXACT, NONLIN, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+      smem_limit(*a.dstate, k_rhs_tiled<EXACT, NONLIN, double2>, (int)smem);
       k_rhs_tiled<EXACT, NONLIN, double2><<<blocks, 32 * RT_WARPS, smem, st>>>(a, a.err);
     }
     return cudaGetLastError();
@@ -521,7 +520,7 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
   if (per * groups > 200 * 1024) return cudaErrorInvalidValue;
   const int T = groups * P;
   size_t smem = per * groups;
-  cudaFuncSetAttribute(k_column<P, EXACT, NONLIN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  smem_limit(*a.dstate, k_column<P, EXACT, NONLIN, MODE>, 200 * 1024);
   int blocks = (g.ncol + groups - 1) / groups;
   k_column<P, EXACT, NONLIN, MODE><<<blocks, T, smem, st>>>(a);
   return cudaGetLastError();
@@ -561,6 +560,7 @@ cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysSca
   a.y = d.y;
   a.gdamp = d.gdamp;
   a.err = d.err;
+  a.dstate = &d;
   {
     const char* e = std::getenv("HST_RHS_TILED");
     a.tiled = !(e && std::atoi(e) == 0);
@@ -611,7 +611,7 @@ static cudaError_t launch_line_solve_t(const Geometry& g, const DeviceState& d, 
   while (groups > 1 && per * groups > 200 * 1024) groups >>= 1;
   if (per * groups > 200 * 1024) return cudaErrorInvalidValue;
   const int T = groups * P;
-  cudaFuncSetAttribute(k_line_solve<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  smem_limit(d, k_line_solve<P>, 200 * 1024);
   int blocks = (g.ncol + groups - 1) / groups;
   k_line_solve<P><<<blocks, T, per * groups, st>>>(g, ph, sys, lambda, d.F[src], d.F[dst], sx, sz, d.der, d.derS);
   return cudaGetLastError();

@@ -23,30 +23,31 @@
 //     stream, or order them with events.
 //   - Nothing in the scratch has to start at zero: every call first rewrites
 //     each entry its solve reads.
-//   - The first call on a device looks up the scratch's device address with
-//     cudaGetSymbolAddress (with that device current); make that first call
-//     before any stream capture begins.
+//   - Every call looks up the scratch's device address with
+//     cudaGetSymbolAddress on the current device (a table lookup, not an
+//     allocation), so that the address is always the one of the context
+//     current now: after cudaDeviceReset, or under another context made
+//     current on the same device, the library's device code is loaded again
+//     and the array may move.  The first call in a context may be the one
+//     that loads that code: make it before any stream capture begins.
+//   - Neither src nor der may overlap dst: the solve reads both while it
+//     writes dst (HST_EARG otherwise).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <cstdarg>
 #include <cstdlib>
 #include <cstdio>
-#include <mutex>
 
 #include "hst_dev.cuh"
 #include "hst_internal.h"
 
 #define HST_NOALLOC_MAX_NY 2048
-#define HST_NOALLOC_MAX_DEVICES 64
 
 namespace {
 
 // der(0:ny-1, 0:3, -2:2) reordered slab-major (the order of hst::SlabDer)
 __device__ __align__(256) double g_line_der[20 * HST_NOALLOC_MAX_NY];
-
-double* g_scratch[HST_NOALLOC_MAX_DEVICES];
-std::mutex g_scratch_lock;
 
 // out[((n*5 + j)*m + i)*P + s] = der(s*m + i, n, j - 2)
 __global__ void k_slab_major(const double* __restrict__ der, double* __restrict__ out, int ny, int P, int m) {
@@ -69,9 +70,11 @@ int fail(char* msg, int len, int rc, const char* fmt, ...) {
   return rc;
 }
 
-// lanes of a solver group: the rule of the context's geometry (the widest
-// power of two up to 32 that leaves at least 8 rows per lane, else 4;
-// HST_LINE_LANES overrides), so both entry points solve identically
+// lanes of a solver group: the rule of the context's default geometry (the
+// widest power of two up to 32 that leaves at least 8 rows per lane, else 4;
+// HST_LINE_LANES overrides), so the results are identical to those of a
+// context that has not been autotuned; hst_gpu_autotune may give a context
+// another group width, and the two then agree up to rounding
 int line_lanes(int ny) {
   const char* env = std::getenv("HST_LINE_LANES");
   if (env) {
@@ -100,10 +103,12 @@ extern "C" int hst_gpu_line_solve_noalloc(int nx, int ny, int nz, double alfa0, 
   if (((uintptr_t)src & 15) || ((uintptr_t)dst & 15) || ((uintptr_t)der & 7))
     return fail(msg, msg_len, HST_EARG, "src/dst must be 16-byte aligned, der 8-byte aligned");
   {
-    // the solve reads src while it writes dst: they must not overlap
+    // the solve reads src and der while it writes dst: neither may overlap it
     const size_t bytes = (size_t)(nx + 1) * (2 * nz + 1) * (ny + 4) * 16;
-    const uintptr_t a = (uintptr_t)src, b = (uintptr_t)dst;
+    const size_t dbytes = (size_t)20 * ny * sizeof(double);
+    const uintptr_t a = (uintptr_t)src, b = (uintptr_t)dst, c = (uintptr_t)der;
     if (a < b + bytes && b < a + bytes) return fail(msg, msg_len, HST_EARG, "src and dst overlap");
+    if (c < b + bytes && b < c + dbytes) return fail(msg, msg_len, HST_EARG, "der and dst overlap");
   }
   const int P = line_lanes(ny);
   if (!P) return fail(msg, msg_len, HST_EARG, "ny = %d: no solver group with at least 4 rows per lane", ny);
@@ -111,21 +116,10 @@ extern "C" int hst_gpu_line_solve_noalloc(int nx, int ny, int nz, double alfa0, 
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(msg, msg_len, HST_ECUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= HST_NOALLOC_MAX_DEVICES)
-    return fail(msg, msg_len, HST_EARG, "device %d out of range (< %d)", dev, HST_NOALLOC_MAX_DEVICES);
-  double* scratch;
-  {
-    std::lock_guard<std::mutex> lk(g_scratch_lock);
-    if (!g_scratch[dev]) {
-      // once per device, with that device current
-      void* p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_line_der);
-      if (e != cudaSuccess)
-        return fail(msg, msg_len, HST_ECUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-      g_scratch[dev] = static_cast<double*>(p);
-    }
-    scratch = g_scratch[dev];
-  }
+  // the scratch's address in the context current now (see the header)
+  double* scratch = nullptr;
+  e = cudaGetSymbolAddress((void**)&scratch, g_line_der);
+  if (e != cudaSuccess) return fail(msg, msg_len, HST_ECUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
 
   hst::Geometry g = {};
   g.nx = nx;

@@ -291,9 +291,12 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
       const C a0 = L(0, x), a1 = L(1, x), b = L(2, x);
       double c0 = fabs((double)a0.x) / ps.dx + fabs((double)a0.y) / rdy0 + fabs((double)b.x) / ps.dz;
       double c1 = fabs((double)a1.x) / ps.dx + fabs((double)a1.y) / rdy1 + fabs((double)b.y) / ps.dz;
-      cm = fmax(cm, fmax(c0, c1));
+      cm = nan_max(cm, nan_max(c0, c1));
     }
-    for (int o = 16; o > 0; o >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+    for (int o = 16; o > 0; o >>= 1) cm = nan_max(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+    // a NaN keeps its bits: as an unsigned word it exceeds every finite
+    // non-negative double and infinity, so it wins the maximum and the host
+    // sees a non-finite CFL number
     if ((threadIdx.x & 31) == 0) atomicMax(cflmax, (unsigned long long)__double_as_longlong(cm));
   }
   // the six product lines, transformed forward in place
@@ -424,8 +427,8 @@ static int fft_threads(int points, int ppt) {
 }
 
 template <typename K>
-static void big_smem(K k) {
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+static void big_smem(const DeviceState& d, K k) {
+  smem_limit(d, k, 220 * 1024);
 }
 
 // Dispatch on the transform length: compile-time plans for the lengths the
@@ -481,10 +484,10 @@ cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st
 #define HST_ZINV(NT, PPT)                                                                                     \
   {                                                                                                           \
     if (NT == 1536) {                                                                                         \
-      big_smem(k_zinv_1536f);                                                                                 \
+      big_smem(d, k_zinv_1536f);                                                                                 \
       k_zinv_1536f<<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], Z, d.twzf);          \
     } else {                                                                                                  \
-      big_smem(k_zinv<NT, PPT, C>);                                                                           \
+      big_smem(d, k_zinv<NT, PPT, C>);                                                                           \
       k_zinv<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], Z, d.twzf);    \
     }                                                                                                         \
   }
@@ -496,7 +499,7 @@ cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st
   const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
 #define HST_ZINV(NT, PPT)                                                                                     \
   {                                                                                                           \
-    big_smem(k_zinv<NT, PPT, C>);                                                                             \
+    big_smem(d, k_zinv<NT, PPT, C>);                                                                             \
     k_zinv<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], d.Z, d.twz);     \
   }
   HST_FFT_DISPATCH(g.nzd, pts, g.pptz == 8, HST_ZINV);
@@ -514,7 +517,7 @@ cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st
     C* Q = reinterpret_cast<C*>(d.Q);
 #define HST_ZFWD(NT, PPT)                                                                  \
   {                                                                                        \
-    big_smem(k_zfwd<NT, PPT, C>);                                                          \
+    big_smem(d, k_zfwd<NT, PPT, C>);                                                          \
     k_zfwd<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, Pp, Q, d.twzf);       \
   }
     HST_FFT_DISPATCH_MP(g.nzd, g.pptz == 16, HST_ZFWD);
@@ -525,7 +528,7 @@ cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st
   const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
 #define HST_ZFWD(NT, PPT)                                                                  \
   {                                                                                        \
-    big_smem(k_zfwd<NT, PPT, C>);                                                          \
+    big_smem(d, k_zfwd<NT, PPT, C>);                                                          \
     k_zfwd<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Pp, d.Q, d.twz);    \
   }
   HST_FFT_DISPATCH(g.nzd, pts, g.pptz == 8, HST_ZFWD);
@@ -547,7 +550,7 @@ cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScal
     C* Pp = reinterpret_cast<C*>(d.Pp);
 #define HST_XPROD(NT, PPT)                                                                                    \
   {                                                                                                           \
-    big_smem(k_xprod<NT, PPT, C>);                                                                            \
+    big_smem(d, k_xprod<NT, PPT, C>);                                                                            \
     k_xprod<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, Z, Pp, d.twxf, d.dyl, ph, want_cfl,     \
                                                                     d.cfl, d.tmZ, d.tmPp, d.err);             \
   }
@@ -559,7 +562,7 @@ cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScal
   const size_t smem = xprod_uses_maps(g) ? xprod_tma_smem(NX, g.nxB, sizeof(C)) : (size_t)6 * (NX + 1) * sizeof(C);
 #define HST_XPROD(NT, PPT)                                                                                    \
   {                                                                                                           \
-    big_smem(k_xprod<NT, PPT, C>);                                                                            \
+    big_smem(d, k_xprod<NT, PPT, C>);                                                                            \
     k_xprod<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Z, d.Pp, d.twx, d.dyl, ph, want_cfl,  \
                                                                     d.cfl, d.tmZ, d.tmPp, d.err);             \
   }

@@ -31,7 +31,16 @@ PI = 3.141592653589793
 
 
 class HstError(RuntimeError):
-    pass
+    """A failed call of the C ABI; `code` is its HST_E* status (0 when the
+    failure was found on the host side of this module)."""
+
+    def __init__(self, msg, code=0):
+        super().__init__(msg)
+        self.code = code
+
+
+# status classes (include/hst_gpu.h)
+EARG, ENOMEM, ECUDA, ETIMEOUT, EFINITE = -1, -2, -3, -4, -5
 
 
 class Params(ct.Structure):
@@ -105,7 +114,7 @@ def lib():
 
 
 # ------------------------------------------------------------------ deck ----
-DECK_DEFAULTS = dict(  # src/hst_input.f90:140-155
+DECK_DEFAULTS = dict(  # src/hst_input.f90:26-42
     nx=63, ny=128, nz=63, alfa0=2.0 * PI / 3.0, beta0=2.0 * PI, ly=2.0, ystretch=0.0,
     re=1000.0, S=1.0, linear=False, exact_shift=False,
     s2_mean=0.0, s2_amplitude=0.0, s2_period=0.0, s2_start=0.0,
@@ -168,7 +177,7 @@ def fft_fit(n: int) -> bool:
 
 
 def padded_sizes(nx, nz, nxd=0, nzd=0):
-    """nxd, nzd as read_input derives them (src/hst_input.f90:210-211)."""
+    """nxd, nzd as read_input derives them (src/hst_input.f90:97-98)."""
     if nxd <= 0:
         nxd = 3 * (nx + 1) // 2
         while not fft_fit(nxd):
@@ -211,7 +220,7 @@ class Solver:
         self._h = ct.c_void_p()
         rc = lib().hst_gpu_create(ct.byref(p), ct.byref(self._h))
         if rc != 0:
-            raise HstError(f"hst_gpu_create failed ({rc}) for nx={p.nx} ny={p.ny} nz={p.nz}")
+            raise HstError(f"hst_gpu_create failed ({rc}) for nx={p.nx} ny={p.ny} nz={p.nz}", rc)
         self.nx, self.ny, self.nz = p.nx, p.ny, p.nz
         self.nxd, self.nzd = padded_sizes(p.nx, p.nz, p.nxd, p.nzd)
         self.shape = (self.nx + 1, 2 * self.nz + 1, self.ny + 4)
@@ -251,7 +260,7 @@ class Solver:
     def _check(self, rc, what):
         if rc != 0:
             msg = lib().hst_gpu_last_error(self._h)
-            raise HstError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+            raise HstError(f"{what} failed ({rc}): {msg.decode() if msg else ''}", rc)
 
     # ---- fields
     def upload(self, field: int, a: np.ndarray):

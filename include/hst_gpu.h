@@ -14,7 +14,8 @@
  *                   s2_integral (src/hst_derivatives.f90:25-26)
  *   hst_fft         device_sync (src/hst_fft.f90:162)
  * The Fortran side (the hst.in deck, the Dati.cart files, the time loop)
- * stays as it is; INTEGRATION.md shows the ISO_C_BINDING interface block.
+ * stays as it is and calls these functions through an ISO_C_BINDING
+ * interface block.
  *
  * Conventions
  *   - Every function returns 0 on success or a negative HST_E* class;
@@ -70,8 +71,8 @@ extern "C" {
 #define HST_KIND_D0 4
 #define HST_KIND_DY 5
 
-/* What the context needs from the deck (src/hst_input.f90:132-137 and the
- * derived quantities :205-215).  nxd, nzd <= 0: derived as the reference
+/* What the context needs from the deck (the namelists of
+ * src/hst_input.f90:19-23 and the derived quantities :92-102).  nxd, nzd <= 0: derived as the reference
  * does (fft_fit).  ystretch: the y grid of src/hst_setup.f90:80-89. */
 typedef struct hst_gpu_params {
   int nx, ny, nz;
@@ -238,8 +239,13 @@ void* hst_gpu_stream(const hst_ctx* ctx);
  * device memory is allocated: the working table lives in a static array of
  * the library, one per device, which limits ny to 2048 (larger ny returns
  * HST_EARG).  Calls on one device must not overlap in time (one stream, or
- * ordered by events).  The first call on a device does set-up (it looks up
- * the static array's address): make it before any stream capture begins.
+ * ordered by events).  Neither src nor der may overlap dst.  Every call looks
+ * up the static array's address in the context current at that moment (a
+ * lookup, not an allocation; a device reset may move the array); the first
+ * call in a context may load the library's device code: make it before any
+ * stream capture begins.  Results equal hst_gpu_line_solve's on a context
+ * that has not been autotuned (hst_gpu_autotune may pick another solver
+ * group width; the two then agree up to rounding).
  * Errors: a negative HST_E* class, with a message in msg[0:msg_len) when msg
  * is not NULL.  No counterpart in the reference, whose line_solve always
  * works on its module arrays (src/hst_linsolve.f90:147). */

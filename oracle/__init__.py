@@ -103,6 +103,7 @@ def lib():
             "ora_damping_active": (i, [vp]),
             "ora_line_solve": (None, [vp, i, d, i, i, i, d, d]),
             "ora_timestep": (None, [vp]),
+            "ora_substep": (None, [vp, i]),
             "ora_start": (None, [vp]),
             "ora_run": (ct.c_long, [vp, ct.c_long]),
             "ora_outstats": (None, [vp, P(d)]),
@@ -122,6 +123,25 @@ def lib():
 def default_params() -> Params:
     p = Params()
     lib().ora_default_params(ct.byref(p))
+    return p
+
+
+def params_from_deck(deck: dict) -> Params:
+    """Oracle parameters from a deck dict (the keys of the hst.in
+    namelists, as hst.read_deck returns them); no restart file is read."""
+    p = default_params()
+    for k in ("nx", "ny", "nz", "seed", "tg_mode"):
+        if k in deck:
+            setattr(p, k, int(deck[k]))
+    for k in ("alfa0", "beta0", "ly", "ystretch", "re", "S", "s2_mean", "s2_amplitude", "s2_period", "s2_start",
+              "deltat", "cflmax", "t_max", "time", "amplitude", "kpeak", "damp_kpar", "damp_kperp", "damp_rate",
+              "damp_edge", "damp_norm", "damp_angle"):
+        if k in deck:
+            setattr(p, k, float(deck[k]))
+    for k in ("linear", "exact_shift", "damp_hard", "damp_mean", "damp_follow"):
+        if k in deck:
+            setattr(p, k, int(bool(deck[k])))
+    p.restart_from_file = 0
     return p
 
 
@@ -278,6 +298,10 @@ class Sim:
 
     def timestep(self):
         lib().ora_timestep(self.h)
+
+    def substep(self, i):
+        """substep i (0, 1, 2) of timestep"""
+        lib().ora_substep(self.h, int(i))
 
     def start(self):
         lib().ora_start(self.h)

@@ -199,7 +199,7 @@ void ora_set_threads(int n) {
 }
 
 void ora_default_params(ora_params* p) {
-  // src/hst_input.f90:140-155
+  // src/hst_input.f90:26-42
   std::memset(p, 0, sizeof(*p));
   p->nx = 63; p->ny = 128; p->nz = 63;
   p->ly = 2.0; p->alfa0 = 2.0 * PI / 3.0; p->beta0 = 2.0 * PI; p->ystretch = 0.0;
@@ -216,7 +216,7 @@ void ora_default_params(ora_params* p) {
 }
 
 // ------------------------------------------------------ deck reader ----
-// A reader for the namelist subset the decks use (src/hst_input.f90:132-171).
+// A reader for the namelist subset the decks use (src/hst_input.f90:19-23, 44-91).
 static std::string lower(std::string s) {
   for (auto& c : s) c = (char)std::tolower((unsigned char)c);
   return s;
@@ -1225,9 +1225,10 @@ void ora_linsolve(ora_sim* s, double lambda) {
   ora_fill_ghosts_now(s, ORA_V3);
 }
 
-// timestep: src/hst_equations.f90:56-87
-void ora_timestep(ora_sim* s) {
-  for (int i = 0; i < 3; ++i) {
+// substep i (0, 1, 2) of timestep: one pass of the loop body of
+// src/hst_equations.f90:58-86
+void ora_substep(ora_sim* s, int i) {
+  {
     const double* ODE = s->RK[i];
     if (!s->p.linear || i == 2) ora_transform_to_physical(s);
     if (i == 2) ora_compute_cfl(s);
@@ -1250,6 +1251,11 @@ void ora_timestep(ora_sim* s) {
       ora_fill_ghosts_now(s, ORA_V3);
     }
   }
+}
+
+// timestep: src/hst_equations.f90:56-87
+void ora_timestep(ora_sim* s) {
+  for (int i = 0; i < 3; ++i) ora_substep(s, i);
 }
 
 // new_timestep: src/hst.f90:163-169 (one rank)

@@ -105,6 +105,8 @@ void ora_damping_mask(ora_sim* s);
 int ora_damping_active(const ora_sim* s);
 void ora_line_solve(ora_sim* s, int sys, double lambda, int src, int dst, int has_shift, double sx, double sz);
 void ora_timestep(ora_sim* s);
+/* substep i = 0, 1, 2 of timestep */
+void ora_substep(ora_sim* s, int i);
 /* the time loop of src/hst.f90:49-133 without output: set-up (initial field
  * or restart), CFL, new_timestep, then up to max_steps steps */
 void ora_start(ora_sim* s);

@@ -7,7 +7,7 @@ them at 1e-10.  They are the golden vectors of this path.  This script
 copies them unchanged (data, not code) and writes their sha256 sums to
 SHA256SUMS so that a test can check the copies.
 
-    python tests/golden/make_fixtures.py [/path/to/reference]
+    python tests/golden/make_fixtures.py /path/to/reference
 """
 import hashlib
 import pathlib
@@ -36,4 +36,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py /path/to/reference (a checkout of the reference project)")
+    main(sys.argv[1])

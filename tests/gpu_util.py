@@ -10,20 +10,7 @@ PI = math.pi
 
 
 def deck_to_oracle(deck: dict) -> "oracle.Params":
-    p = oracle.default_params()
-    for k in ("nx", "ny", "nz", "seed", "tg_mode"):
-        if k in deck:
-            setattr(p, k, int(deck[k]))
-    for k in ("alfa0", "beta0", "ly", "ystretch", "re", "S", "s2_mean", "s2_amplitude", "s2_period", "s2_start",
-              "deltat", "cflmax", "t_max", "time", "amplitude", "kpeak", "damp_kpar", "damp_kperp", "damp_rate",
-              "damp_edge", "damp_norm", "damp_angle"):
-        if k in deck:
-            setattr(p, k, float(deck[k]))
-    for k in ("linear", "exact_shift", "damp_hard", "damp_mean", "damp_follow"):
-        if k in deck:
-            setattr(p, k, int(bool(deck[k])))
-    p.restart_from_file = 0
-    return p
+    return oracle.params_from_deck(deck)
 
 
 def interior(a):

@@ -82,6 +82,16 @@ def test_async_io_and_noalloc_reject_bad_arguments():
     assert f(15, 4096, 15, 1.0, 1.0, 100.0, 1, 1.0, 16, 32, 64, 0.0, 0.0, None, msg, 128) == -1
     assert b"scratch" in msg.value
     assert f(15, 31, 15, 1.0, 1.0, 100.0, 1, 1.0, 16, 32, 64, 0.0, 0.0, None, msg, 128) == -1
+    # overlaps of dst with src or with der are refused before any CUDA call
+    # (the addresses are never dereferenced)
+    field = 16 * 16 * 31 * 36
+    base = 1 << 32
+    assert f(15, 32, 15, 1.0, 1.0, 100.0, 1, 1.0, base, base + 2 * field, base + 2 * field + 256, 0.0, 0.0, None, msg,
+             128) == -1
+    assert b"src and dst" in msg.value
+    assert f(15, 32, 15, 1.0, 1.0, 100.0, 1, 1.0, base + 2 * field + 1024, base, base + 2 * field, 0.0, 0.0, None,
+             msg, 128) == -1
+    assert b"der and dst" in msg.value
 
 
 def test_mixed_precision_rejects_uncompiled_sizes():

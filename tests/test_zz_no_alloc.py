@@ -75,3 +75,39 @@ def test_noalloc_rejects_oversize_and_overlap():
     assert rc == -1 and "scratch" in msg
     rc, msg = call(f, deck, hst.KIND_D0, 0.0, der, src, src, (0.0, 0.0), None)
     assert rc == -1 and "overlap" in msg
+
+
+def test_noalloc_at_the_largest_size():
+    """ny = 2048, the largest size the static scratch holds (all of it used,
+    the widest solver group: 32 lanes of 64 rows), one Fourier column pair
+    (nx = nz = 1): every kind against the context's hst_gpu_line_solve, two
+    calls in a row."""
+    import torch
+
+    deck = dict(nx=1, ny=2048, nz=1, alfa0=1.0, beta0=1.0, ly=6.283185307179586, re=1000.0)
+    s = hst.Solver(deck)
+    t = 0.37
+    shift = s.shear_shifts(t)
+    rng = np.random.default_rng(11)
+    V = rng.standard_normal(s.shape) + 1j * rng.standard_normal(s.shape)
+    s.upload(hst.V2, V)
+    s.fill_ghosts(hst.V2, *shift)
+    src_h = s.download(hst.V2)
+    dev = torch.device("cuda:0")
+    src = torch.from_numpy(src_h).to(dev)
+    der = torch.from_numpy(np.ascontiguousarray(s.der).ravel()).to(dev)
+    f = noalloc()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for kind, lam in ((hst.KIND_D2V, 2.5e4), (hst.KIND_ETA, 3.0e3), (hst.KIND_POISSON, 0.0), (hst.KIND_D0, 0.0),
+                      (hst.KIND_DY, 0.0)):
+        s.line_solve(kind, lam, hst.V2, hst.RHS1, shift=shift)
+        want = s.download(hst.RHS1)
+        outs = [torch.zeros_like(src), torch.zeros_like(src)]
+        for out in outs:
+            rc, msg = call(f, deck, kind, lam, der, src, out, shift, stream)
+            assert rc == 0, msg
+        torch.cuda.synchronize(dev)
+        for out in outs:
+            err = rel_l2(out.cpu().numpy(), want)
+            assert err <= TOL, (kind, err)
+    s.close()
