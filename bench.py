@@ -437,11 +437,19 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="precision of the ensemble members (--config c4)")
+    ap.add_argument("--sizes", default=None,
+                    help="NX,NY,NZ: the workload's deck with other sizes (a smaller case of the same kernels, "
+                         "for profiler captures); no CPU leg")
     args = ap.parse_args()
     if args.config == "c4":
         return ensemble_main(args)
     cfg = CONFIGS[args.config]
     cfg = dict(cfg, cpu_baseline=ORACLE_SUBSTEPS[args.config] > 0)
+    if args.sizes:
+        nx, ny, nz = (int(v) for v in args.sizes.split(","))
+        cfg = dict(cfg, deck=dict(cfg["deck"], nx=nx, ny=ny, nz=nz), cpu_baseline=False,
+                   label=cfg["label"] + f"; sizes replaced by nx={nx}, ny={ny}, nz={nz}")
+        args.no_cpu_baseline = True
     if args.impl == "reference":
         return reference_main(args, cfg)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -15,7 +15,7 @@ PKG = pathlib.Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libhst_gpu.so"
-SOURCES = ["hst_kernels.cu", "hst_transforms.cu", "hst_capi.cu", "hst_noalloc.cu", "hst_stats.cu"]
+SOURCES = ["hst_kernels.cu", "hst_transforms.cu", "hst_capi.cu", "hst_noalloc.cu", "hst_stats.cu", "hst_pieces.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

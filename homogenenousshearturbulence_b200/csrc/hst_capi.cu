@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <cstdint>
 #include <new>
 #include <string>
 #include <unordered_set>
@@ -163,6 +164,14 @@ struct hst_ctx {
   cudaEvent_t ev_main = nullptr, ev_in = nullptr, ev_stage = nullptr, ev_out = nullptr;
   double2* snap[3] = {nullptr, nullptr, nullptr};
   double2* stage[3] = {nullptr, nullptr, nullptr};
+  // host address ranges registered by the caller (hst_gpu_register_host): a
+  // Fortran array's base address -> field or buffer-component id
+  struct HostRange {
+    uintptr_t base;
+    size_t bytes;
+    int id;
+  };
+  std::vector<HostRange> host_ranges;
   cudaEvent_t ev_staged[3] = {nullptr, nullptr, nullptr};  // stage[c] copied into V (solver's stream)
   cudaEvent_t ev_read[3] = {nullptr, nullptr, nullptr};    // snap[c] copied to the host (copy-out stream)
   bool staged_used[3] = {false, false, false}, read_used[3] = {false, false, false};
@@ -406,7 +415,8 @@ static void free_device(hst_ctx* c) {
   DeviceState& d = c->d;
   for (int i = 0; i < 7; ++i)
     if (d.F[i]) cudaFree(d.F[i]);
-  void* ps[] = {d.Z, d.Pp, d.Q, d.der, d.derS, d.d0tab, d.y, d.dyl, d.gdamp, d.twx, d.twz, d.twxf, d.twzf, d.cfl, d.stats};
+  void* ps[] = {d.Z,    d.Pp,  d.Q,    d.der,   d.derS, d.d0tab, d.y,    d.dyl,  d.gdamp,
+                d.twx,  d.twz, d.twxf, d.twzf,  d.cfl,  d.stats, d.vvdz, d.vvdx, d.vvdp};
   for (void* q : ps)
     if (q) cudaFree(q);
   std::memset(&d, 0, sizeof d);
@@ -510,7 +520,7 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   ok = ok && alloc((void**)&d.twxf, sizeof(float2) * 4 * g.nxd);
   ok = ok && alloc((void**)&d.twzf, sizeof(float2) * g.nzd);
   // outstats scratch (sized for the largest reduction grid, 4 blocks an SM of up to 256 SMs)
-  ok = ok && alloc((void**)&d.stats, sizeof(double) * (13 * 4 * 256 + 8));
+  ok = ok && alloc((void**)&d.stats, sizeof(double) * ((hst::stats_partials() + 3) * 4 * 256 + 24));
   // two words: the CFL maximum and the bounded-wait error flag
   ok = ok && alloc((void**)&d.cfl, 2 * sizeof(unsigned long long));
   if (ok) d.err = reinterpret_cast<int*>(d.cfl + 1);
@@ -800,15 +810,16 @@ extern "C" int hst_gpu_compute_cfl(hst_ctx* ctx, double* cfl) {
 
 // outstats (src/hst_stats.f90:136-285) of the resident field at `time`:
 // the three DY solves go through RHS1, which is scratch between steps (as
-// the reference's rhs is)
-extern "C" int hst_gpu_outstats(hst_ctx* ctx, double time, double* out) {
-  if (!ctx || !out) return HST_EARG;
+// the reference's rhs is).  res (24 doubles on the host): the 8 box averages,
+// then the 16 sums of the reference's `sums` array; exz (ncol doubles, may
+// be NULL): the column energies, computed into RHS1 after the solves.
+static int outstats_all(hst_ctx* ctx, double time, double* res_h, double* exz_h) {
   CK(cudaSetDevice(ctx->device));
   const Geometry& g = ctx->g;
   const int nblk = hst::stats_blocks(g, ctx->d.nsm);
   if (nblk > 4 * 256) return fail(ctx, HST_EARG, "outstats: %d reduction blocks exceed the scratch", nblk);
   double* pm = ctx->d.stats;
-  double* pg = pm + (size_t)9 * nblk;
+  double* pg = pm + (size_t)hst::stats_partials() * nblk;
   double* res = pg + (size_t)3 * nblk;
   double sx, sz;
   shear_shifts(ctx, time, &sx, &sz);
@@ -819,13 +830,43 @@ extern "C" int hst_gpu_outstats(hst_ctx* ctx, double time, double* out) {
     CK(hst::launch_stats_grad(g, ctx->d, HST_RHS1, pg + (size_t)c * nblk, ctx->stream));
     ctx->launches++;
   }
-  CK(hst::launch_stats_moments(g, ctx->d, ctx->ps, pm, ctx->stream));
+  const double gsoft = (damping_active(ctx->p) && !ctx->p.damp_hard) ? 1.0 : 0.0;
+  CK(hst::launch_stats_moments(g, ctx->d, ctx->ps, gsoft, pm, ctx->stream));
   double ly_w = 0.0;
   for (int iy = 0; iy < g.ny; ++iy) ly_w += ctx->dyl[iy];
   CK(hst::launch_stats_final(g, ctx->d, pm, pg, ly_w, ctx->ps.ni, ctx->p.ly, res, ctx->stream));
   ctx->launches += 2;
-  CK(cudaMemcpyAsync(out, res, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  double* exz_d = reinterpret_cast<double*>(ctx->d.F[HST_RHS1]);
+  if (exz_h) {
+    CK(hst::launch_stats_columns(g, ctx->d, exz_d, ctx->stream));
+    ctx->launches++;
+  }
+  CK(cudaMemcpyAsync(res_h, res, 24 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (exz_h) CK(cudaMemcpyAsync(exz_h, exz_d, sizeof(double) * g.ncol, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  // ncol_damped (src/hst_damping.f90:113): the columns of the current table
+  int n = 0;
+  if (damping_active(ctx->p))
+    for (double v : ctx->gdamp) n += v > 0.0;
+  res_h[8 + 15] = (double)n;
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_outstats(hst_ctx* ctx, double time, double* out) {
+  if (!ctx || !out) return HST_EARG;
+  double res[24];
+  int rc = outstats_all(ctx, time, res, nullptr);
+  if (rc != HST_OK) return rc;
+  std::memcpy(out, res, 8 * sizeof(double));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_outstats_sums(hst_ctx* ctx, double time, double* sums, double* exz) {
+  if (!ctx || !sums) return HST_EARG;
+  double res[24];
+  int rc = outstats_all(ctx, time, res, exz);
+  if (rc != HST_OK) return rc;
+  std::memcpy(sums, res + 8, 16 * sizeof(double));
   return HST_OK;
 }
 
@@ -1179,4 +1220,328 @@ extern "C" int hst_gpu_reset_kernel_times(hst_ctx* ctx) {
     ctx->prof_n[k] = 0;
   }
   return HST_OK;
+}
+
+// ------------------------------------------------- the substep in pieces ----
+// The module procedures of hst_transforms, hst_fft and hst_equations one at
+// a time, on buffers in the reference's layouts (hst_pieces.cu), for callers
+// that run the substep's pieces themselves.  The buffers are allocated by the
+// first call that needs them.
+static size_t piece_comp_elems(const Geometry& g, int buf) {
+  return buf == HST_BUF_VVDZ ? (size_t)g.rows * g.nxB * g.nzd : (size_t)g.rows * g.nzd * (g.nxd + 1);
+}
+static double2* piece_buf(hst_ctx* ctx, int buf) {
+  return buf == HST_BUF_VVDZ ? ctx->d.vvdz : (buf == HST_BUF_VVDX ? ctx->d.vvdx : ctx->d.vvdp);
+}
+
+static int ensure_pieces(hst_ctx* ctx) {
+  if (ctx->d.vvdz) return HST_OK;
+  CK(cudaSetDevice(ctx->device));
+  const Geometry& g = ctx->g;
+  double2** bufs[3] = {&ctx->d.vvdz, &ctx->d.vvdx, &ctx->d.vvdp};
+  for (int b = 0; b < 3; ++b) {
+    const size_t bytes = sizeof(double2) * 3 * piece_comp_elems(g, b);
+    if (cudaMalloc((void**)bufs[b], bytes) != cudaSuccess) {
+      cudaGetLastError();
+      for (int k = 0; k < 3; ++k)
+        if (*bufs[k]) cudaFree(*bufs[k]);
+      ctx->d.vvdz = ctx->d.vvdx = ctx->d.vvdp = nullptr;
+      return fail(ctx, HST_ENOMEM, "the per-piece buffers (3 x %.2f GB) were refused",
+                  3.0 * sizeof(double2) * piece_comp_elems(g, 1) / 1e9);
+    }
+    CK(cudaMemsetAsync(*bufs[b], 0, bytes, ctx->stream));
+  }
+  return HST_OK;
+}
+
+static int check_m(hst_ctx* ctx, int m, const char* what) {
+  if (m < 1 || m > 3) return fail(ctx, HST_EARG, "%s: component m = %d, expected 1..3", what, m);
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_fft(hst_ctx* ctx, int kind, int m) {
+  if (!ctx) return HST_EARG;
+  int rc = check_m(ctx, m, "fft");
+  if (rc == HST_OK) rc = ensure_pieces(ctx);
+  if (rc != HST_OK) return rc;
+  const Geometry& g = ctx->g;
+  const hst::DeviceState& d = ctx->d;
+  const int c = m - 1;
+  if (kind == HST_FFT_FFT || kind == HST_FFT_IFT) {
+    const size_t ce = piece_comp_elems(g, HST_BUF_VVDZ);
+    CK(hst::launch_piece_lines(d, d.vvdz + c * ce, g.nzd, g.rows * g.nxB, g.nzd, 0, kind == HST_FFT_IFT ? +1 : -1,
+                               d.twz, ctx->stream));
+  } else if (kind == HST_FFT_RFT) {
+    const size_t ce = piece_comp_elems(g, HST_BUF_VVDX);
+    CK(hst::launch_piece_lines(d, d.vvdx + c * ce, g.nxd + 1, g.rows * g.nzd, 2 * g.nxd, 1, +1, d.twx, ctx->stream));
+  } else if (kind == HST_FFT_HFT) {
+    const size_t ce = piece_comp_elems(g, HST_BUF_VVDP);
+    CK(hst::launch_piece_lines(d, d.vvdp + c * ce, g.nxd + 1, g.rows * g.nzd, 2 * g.nxd, 2, -1, d.twx, ctx->stream));
+  } else {
+    return fail(ctx, HST_EARG, "fft: unknown kind %d", kind);
+  }
+  ctx->launches++;
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_transpose(hst_ctx* ctx, int dir, int m) {
+  if (!ctx) return HST_EARG;
+  int rc = check_m(ctx, m, "transpose");
+  if (rc == HST_OK) rc = ensure_pieces(ctx);
+  if (rc != HST_OK) return rc;
+  if (dir != HST_Z_TO_X && dir != HST_X_TO_Z) return fail(ctx, HST_EARG, "transpose: unknown direction %d", dir);
+  CK(hst::launch_transpose(ctx->g, ctx->d, dir == HST_Z_TO_X, m - 1, ctx->stream));
+  ctx->launches++;
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_transform_to_physical(hst_ctx* ctx) {
+  if (!ctx) return HST_EARG;
+  int rc = ensure_pieces(ctx);
+  if (rc != HST_OK) return rc;
+  CK(cudaSetDevice(ctx->device));
+  CK(hst::launch_assemble_vvdz(ctx->g, ctx->d, ctx->stream));
+  ctx->launches++;
+  for (int m = 1; m <= 3 && rc == HST_OK; ++m) {
+    rc = hst_gpu_fft(ctx, HST_FFT_IFT, m);
+    if (rc == HST_OK) rc = hst_gpu_transpose(ctx, HST_Z_TO_X, m);
+    if (rc == HST_OK) rc = hst_gpu_fft(ctx, HST_FFT_RFT, m);
+  }
+  return rc;
+}
+
+extern "C" int hst_gpu_build_products(hst_ctx* ctx, int grp) {
+  if (!ctx) return HST_EARG;
+  if (grp != 1 && grp != 2) return fail(ctx, HST_EARG, "build_products: group %d, expected 1 or 2", grp);
+  int rc = ensure_pieces(ctx);
+  if (rc != HST_OK) return rc;
+  CK(cudaSetDevice(ctx->device));
+  CK(hst::launch_build_products(ctx->g, ctx->d, ctx->ps, grp, ctx->stream));
+  ctx->launches++;
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_products_to_spectral(hst_ctx* ctx) {
+  if (!ctx) return HST_EARG;
+  int rc = ensure_pieces(ctx);
+  for (int m = 1; m <= 3 && rc == HST_OK; ++m) {
+    rc = hst_gpu_fft(ctx, HST_FFT_HFT, m);
+    if (rc == HST_OK) rc = hst_gpu_transpose(ctx, HST_X_TO_Z, m);
+    if (rc == HST_OK) rc = hst_gpu_fft(ctx, HST_FFT_FFT, m);
+  }
+  return rc;
+}
+
+extern "C" int hst_gpu_vvdz_to_field(hst_ctx* ctx, int field, int m) {
+  if (!ctx || field < 0 || field > 6) return fail(ctx, HST_EARG, "vvdz_to_field: bad field %d", field);
+  int rc = check_m(ctx, m, "vvdz_to_field");
+  if (rc == HST_OK) rc = ensure_pieces(ctx);
+  if (rc != HST_OK) return rc;
+  CK(cudaSetDevice(ctx->device));
+  CK(hst::launch_vvdz_to_field(ctx->g, ctx->d, m - 1, field, ctx->stream));
+  ctx->launches++;
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_buildrhs_prepare(hst_ctx* ctx, const double* ODE, double deltat, double time) {
+  if (!ctx || !ODE || !(deltat > 0.0)) return fail(ctx, HST_EARG, "buildrhs_prepare: bad arguments");
+  CK(cudaSetDevice(ctx->device));
+  const hst_gpu_params& p = ctx->p;
+  SubstepScalars sc = {};
+  sc.ode0 = ODE[0];
+  sc.ode1 = ODE[1];
+  sc.ode2 = ODE[2];
+  sc.deltat = deltat;
+  sc.lambda = ODE[0] / deltat;
+  sc.s2now = s2_of(p, time);
+  sc.gsoft = (damping_active(p) && !p.damp_hard) ? 1.0 : 0.0;
+  sc.damp_hard = 0;  // the mask is its own piece (hst_gpu_damping_mask)
+  shear_shifts(ctx, time, &sc.sx_t, &sc.sz_t);
+  CK(timed(ctx, HST_KC_RHS,
+           [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, 1, 0, 4, ctx->stream); }));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_buildrhs(hst_ctx* ctx, const double* ODE, int grp) {
+  if (!ctx || !ODE || (grp != 1 && grp != 2)) return fail(ctx, HST_EARG, "buildrhs: bad arguments");
+  int rc = ensure_pieces(ctx);
+  if (rc != HST_OK) return rc;
+  CK(cudaSetDevice(ctx->device));
+  CK(hst::launch_buildrhs_group(ctx->g, ctx->d, ctx->ps, ODE[1], grp, ctx->stream));
+  ctx->launches++;
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_damping_update(hst_ctx* ctx, double time) {
+  if (!ctx) return HST_EARG;
+  if (!damping_active(ctx->p) || !damping_update(ctx, time)) return HST_OK;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::memcpy(ctx->h_gdamp, ctx->gdamp.data(), sizeof(double) * ctx->g.ncol);
+  CK(cudaMemcpyAsync(ctx->d.gdamp, ctx->h_gdamp, sizeof(double) * ctx->g.ncol, cudaMemcpyHostToDevice, ctx->stream));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_damping_mask(hst_ctx* ctx) {
+  if (!ctx) return HST_EARG;
+  if (!(ctx->p.damp_hard && damping_active(ctx->p))) return HST_OK;
+  CK(cudaSetDevice(ctx->device));
+  CK(hst::launch_damping_mask(ctx->g, ctx->d, ctx->stream));
+  ctx->launches++;
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_shear_shift(hst_ctx* ctx, double dt_sub, double time) {
+  if (!ctx) return HST_EARG;
+  CK(cudaSetDevice(ctx->device));
+  const hst_gpu_params& p = ctx->p;
+  const double dgx = p.S * dt_sub, dgz = s2_integral(p, time, time + dt_sub);
+  if (!p.exact_shift) {
+    CK(hst::launch_shift_default(ctx->g, ctx->d, ctx->ps, dgx, dgz, ctx->stream));
+    ctx->launches++;
+    return HST_OK;
+  }
+  SubstepScalars sc = {};
+  sc.dgx = dgx;
+  sc.dgz = dgz;
+  sc.yuni = p.ystretch <= 1.0e-10 ? 1 : 0;
+  sc.ytile = p.ly * 32.0 / p.ny;
+  shear_shifts(ctx, time, &sc.sx_t, &sc.sz_t);
+  shear_shifts(ctx, time + dt_sub, &sc.sx_n, &sc.sz_n);
+  CK(timed(ctx, HST_KC_COLUMN, [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, 1, 0, 3, ctx->stream); }));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_linsolve(hst_ctx* ctx, double lambda, double time) {
+  if (!ctx) return HST_EARG;
+  CK(cudaSetDevice(ctx->device));
+  SubstepScalars sc = {};
+  sc.lambda = lambda;
+  shear_shifts(ctx, time, &sc.sx_n, &sc.sz_n);
+  CK(timed(ctx, HST_KC_COLUMN,
+           [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, 0, !ctx->p.linear, 2, ctx->stream); }));
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_buffer_pointer(hst_ctx* ctx, int buf, void** dptr, size_t* bytes) {
+  if (!ctx || buf < HST_BUF_VVDZ || buf > HST_BUF_VVDP || !dptr) return fail(ctx, HST_EARG, "buffer_pointer: bad buffer");
+  int rc = ensure_pieces(ctx);
+  if (rc != HST_OK) return rc;
+  *dptr = piece_buf(ctx, buf);
+  if (bytes) *bytes = sizeof(double2) * 3 * piece_comp_elems(ctx->g, buf);
+  return HST_OK;
+}
+
+static int buffer_copy(hst_ctx* ctx, int buf, int m, void* host, bool up) {
+  if (!ctx || buf < HST_BUF_VVDZ || buf > HST_BUF_VVDP || !host) return fail(ctx, HST_EARG, "buffer copy: bad buffer");
+  int rc = check_m(ctx, m, "buffer copy");
+  if (rc == HST_OK) rc = ensure_pieces(ctx);
+  if (rc != HST_OK) return rc;
+  CK(cudaSetDevice(ctx->device));
+  const size_t ce = piece_comp_elems(ctx->g, buf);
+  double2* dev = piece_buf(ctx, buf) + (size_t)(m - 1) * ce;
+  if (up) CK(cudaMemcpyAsync(dev, host, sizeof(double2) * ce, cudaMemcpyHostToDevice, ctx->stream));
+  else CK(cudaMemcpyAsync(host, dev, sizeof(double2) * ce, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return HST_OK;
+}
+extern "C" int hst_gpu_buffer_upload(hst_ctx* ctx, int buf, int m, const double* host) {
+  return buffer_copy(ctx, buf, m, const_cast<double*>(host), true);
+}
+extern "C" int hst_gpu_buffer_download(hst_ctx* ctx, int buf, int m, double* host) {
+  return buffer_copy(ctx, buf, m, host, false);
+}
+
+// -------------------------------------------------- host address registry ----
+static size_t id_bytes(const hst_ctx* ctx, int id) {
+  if (id >= HST_V1 && id <= HST_RHS2) return sizeof(double2) * ctx->g.nf;
+  if (id >= HST_ID_BUF(HST_BUF_VVDZ, 1) && id <= HST_ID_BUF(HST_BUF_VVDP, 3))
+    return sizeof(double2) * piece_comp_elems(ctx->g, (id - HST_ID_BUF(0, 1)) / 3);
+  return 0;
+}
+
+extern "C" int hst_gpu_register_host(hst_ctx* ctx, const void* host, size_t bytes, int id) {
+  if (!ctx || !host) return HST_EARG;
+  const size_t need = id_bytes(ctx, id);
+  if (!need) return fail(ctx, HST_EARG, "register_host: unknown id %d", id);
+  if (bytes != need)
+    return fail(ctx, HST_EARG, "register_host: id %d holds %zu bytes, the host array %zu", id, need, bytes);
+  const uintptr_t b = (uintptr_t)host;
+  for (auto& r : ctx->host_ranges)
+    if (b < r.base + r.bytes && r.base < b + bytes) {
+      if (r.base == b && r.bytes == bytes) {  // the same array again: its id is replaced
+        r.id = id;
+        return HST_OK;
+      }
+      return fail(ctx, HST_EARG, "register_host: the array overlaps one registered as id %d", r.id);
+    }
+  ctx->host_ranges.push_back({b, bytes, id});
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_unregister_host(hst_ctx* ctx, const void* host) {
+  if (!ctx) return HST_EARG;
+  for (size_t k = 0; k < ctx->host_ranges.size(); ++k)
+    if (ctx->host_ranges[k].base == (uintptr_t)host) {
+      ctx->host_ranges.erase(ctx->host_ranges.begin() + (long)k);
+      return HST_OK;
+    }
+  return fail(ctx, HST_EARG, "unregister_host: the address is not registered");
+}
+
+extern "C" int hst_gpu_host_id(const hst_ctx* ctx, const void* host) {
+  if (!ctx) return HST_EARG;
+  for (const auto& r : ctx->host_ranges)
+    if (r.base == (uintptr_t)host) return r.id;
+  return HST_EARG;
+}
+
+static int resolve(hst_ctx* ctx, const void* host, bool fields_only, const char* what) {
+  const int id = hst_gpu_host_id(ctx, host);
+  if (id < 0 || (fields_only && id > HST_RHS2))
+    return fail(ctx, HST_EARG, "%s: the host array at %p is not registered%s", what, host,
+                fields_only ? " as a field" : "");
+  return id;
+}
+
+extern "C" int hst_gpu_upload_host(hst_ctx* ctx, const void* host) {
+  if (!ctx) return HST_EARG;
+  const int id = resolve(ctx, host, false, "upload_host");
+  if (id < 0) return id;
+  if (id <= HST_RHS2) return hst_gpu_upload(ctx, id, static_cast<const double*>(host));
+  const int k = id - HST_ID_BUF(0, 1);
+  return hst_gpu_buffer_upload(ctx, k / 3, k % 3 + 1, static_cast<const double*>(host));
+}
+
+extern "C" int hst_gpu_download_host(hst_ctx* ctx, void* host) {
+  if (!ctx) return HST_EARG;
+  const int id = resolve(ctx, host, false, "download_host");
+  if (id < 0) return id;
+  if (id <= HST_RHS2) return hst_gpu_download(ctx, id, static_cast<double*>(host));
+  const int k = id - HST_ID_BUF(0, 1);
+  return hst_gpu_buffer_download(ctx, k / 3, k % 3 + 1, static_cast<double*>(host));
+}
+
+extern "C" int hst_gpu_line_solve_host(hst_ctx* ctx, int sys, double lambda, const void* src, void* dst, int has_shift,
+                                       double shift_x, double shift_z, double time) {
+  if (!ctx) return HST_EARG;
+  const int a = resolve(ctx, src, true, "line_solve_host src");
+  if (a < 0) return a;
+  const int b = resolve(ctx, dst, true, "line_solve_host dst");
+  if (b < 0) return b;
+  return hst_gpu_line_solve(ctx, sys, lambda, a, b, has_shift, shift_x, shift_z, time);
+}
+
+extern "C" int hst_gpu_fill_ghosts_host(hst_ctx* ctx, void* field, double shift_x, double shift_z) {
+  if (!ctx) return HST_EARG;
+  const int a = resolve(ctx, field, true, "fill_ghosts_host");
+  if (a < 0) return a;
+  return hst_gpu_fill_ghosts(ctx, a, shift_x, shift_z);
+}
+
+extern "C" int hst_gpu_vvdz_to_field_host(hst_ctx* ctx, void* field, int m) {
+  if (!ctx) return HST_EARG;
+  const int a = resolve(ctx, field, true, "vvdz_to_field_host");
+  if (a < 0) return a;
+  return hst_gpu_vvdz_to_field(ctx, a, m);
 }

@@ -46,8 +46,11 @@ struct DeviceState {
   CUtensorMap tmZ, tmPp;
   bool maps;
   int nsm;        // SMs of the device
-  double* stats;  // outstats scratch: block partials of the moments (9 a block), of the three
-                  // gradients (one a block each), then the 8 results
+  double* stats;  // outstats scratch: block partials of the moments (stats_partials() a block),
+                  // of the three gradients (one a block each), then the 24 results
+  // the reference-layout buffers of the per-piece path (allocated by its
+  // first call): VVdz [3][ny+4][nx+1][nzd], VVdx and VVdp [3][ny+4][nzd][nxd+1]
+  double2 *vvdz, *vvdx, *vvdp;
   // kernels whose shared-memory limit has been raised in this context
   // (owned by the context; null: raise it at every launch)
   std::unordered_set<const void*>* configured;
@@ -86,7 +89,9 @@ cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st
 cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int want_cfl, cudaStream_t st);
 cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st);
 // part: 0 the fused column kernel, 1 its right-hand-side stage alone (row
-// streaming, into RHS1/RHS2), 2 the rest (shift, solves, u, w) from RHS1/RHS2
+// streaming, into RHS1/RHS2), 2 the rest (shift, solves, u, w) from RHS1/RHS2,
+// 3 (exact only, nonlin 0) the exact_shift shift of RHS1/2, OLD1/2 alone,
+// 4 the right-hand-side stage in its untiled FP64 form
 cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysScalars& ph, const SubstepScalars& sc,
                           int exact, int nonlin, int part, cudaStream_t st);
 cudaError_t launch_line_solve(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int sys, double lambda,
@@ -101,8 +106,12 @@ size_t d0_table_doubles(int ny);
 // outstats (src/hst_stats.f90:136-285): block count of the reductions and
 // the three kernels (hst_stats.cu)
 int stats_blocks(const Geometry& g, int nsm);
-cudaError_t launch_stats_moments(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double* partial,
-                                 cudaStream_t st);
+cudaError_t launch_stats_moments(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double gsoft,
+                                 double* partial, cudaStream_t st);
+// the column energies exz(-nz:nz, 0:nx) of outstats into exz (ncol doubles)
+cudaError_t launch_stats_columns(const Geometry& g, const DeviceState& d, double* exz, cudaStream_t st);
+// moment partials a reduction block writes
+int stats_partials();
 cudaError_t launch_stats_grad(const Geometry& g, const DeviceState& d, int field, double* partial, cudaStream_t st);
 cudaError_t launch_stats_final(const Geometry& g, const DeviceState& d, const double* pm, const double* pg,
                                double ly_w, double ni, double ly, double* out, cudaStream_t st);
@@ -112,6 +121,20 @@ cudaError_t launch_stats_final(const Geometry& g, const DeviceState& d, const do
 cudaError_t launch_pressure_rhs(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double s2now,
                                 double sx, double sz, cudaStream_t st);
 cudaError_t launch_pressure_mean(const Geometry& g, const DeviceState& d, double ly, int dst, cudaStream_t st);
+// the per-piece path (hst_pieces.cu; the line transforms in hst_transforms.cu):
+// kind 0 z line, 1 c2r x line, 2 r2c x line; S the sign of the exponent
+cudaError_t launch_piece_lines(const DeviceState& d, double2* base, size_t stride, int nlines, int N, int kind, int S,
+                               const double2* tw, cudaStream_t st);
+cudaError_t launch_assemble_vvdz(const Geometry& g, const DeviceState& d, cudaStream_t st);
+cudaError_t launch_transpose(const Geometry& g, const DeviceState& d, int to_x, int m, cudaStream_t st);
+cudaError_t launch_build_products(const Geometry& g, const DeviceState& d, const PhysScalars& ps, int grp,
+                                  cudaStream_t st);
+cudaError_t launch_vvdz_to_field(const Geometry& g, const DeviceState& d, int m, int field, cudaStream_t st);
+cudaError_t launch_buildrhs_group(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double ode2,
+                                  int grp, cudaStream_t st);
+cudaError_t launch_damping_mask(const Geometry& g, const DeviceState& d, cudaStream_t st);
+cudaError_t launch_shift_default(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double dgx,
+                                 double dgz, cudaStream_t st);
 // the TMA maps of Z and Pp for the x kernel (d.maps false when not used)
 cudaError_t make_transform_maps(const Geometry& g, DeviceState& d);
 // the stage-ordered twiddles of the 8-point plan of N into out (at most N

@@ -73,7 +73,9 @@ __device__ __forceinline__ void store_with_ghosts(double2* __restrict__ col, con
 // MODE 0: everything in one kernel.  MODE 1: only the right-hand sides,
 // streamed row by row (P = 32 lanes walk the rows of one column; no shared
 // memory), written to RHS1/RHS2.  MODE 2: the rest, reading RHS1/RHS2.
-enum { COL_FUSED = 0, COL_RHS = 1, COL_SOLVE = 2 };
+// MODE 3 (EXACT only): the exact_shift shear shift of RHS1/2 and OLD1/2 in
+// place and nothing else (the per-piece shear_shift).
+enum { COL_FUSED = 0, COL_RHS = 1, COL_SOLVE = 2, COL_SHIFT = 3 };
 
 template <int P, bool EXACT, bool NONLIN, int MODE>
 __global__ void k_column(ColumnArgs a) {
@@ -115,7 +117,7 @@ __global__ void k_column(ColumnArgs a) {
   const SlabDer DS = {a.derS, g.m, P};
 
   // ---- right-hand sides, row by row (buildrhs_prepare :92-141, buildrhs :151-213)
-  if (MODE != COL_SOLVE) {
+  if (MODE == COL_FUSED || MODE == COL_RHS) {
     const ColConst cc = col_const(col, g, a.ps, sc, a.gdamp);
     const double2* Qc = a.Q + (size_t)col * ny;
     const size_t qs = (size_t)g.ncol * ny;
@@ -150,7 +152,7 @@ __global__ void k_column(ColumnArgs a) {
   // loads and the phases.
   const double th0 = al * sc.sx_t + be * sc.sz_t;
   double2* scr = a.V1 + (size_t)col * g.rows;
-  if (MODE == COL_SOLVE && EXACT) {
+  if ((MODE == COL_SOLVE || MODE == COL_SHIFT) && EXACT) {
     const double gx = al * sc.dgx + be * sc.dgz;
     const cxd phs = cexpi(-(al * sc.sx_n + be * sc.sz_n));
     double2* scr2 = a.V3 + (size_t)col * g.rows;
@@ -192,6 +194,9 @@ __global__ void k_column(ColumnArgs a) {
         if (pass == 0) {
           a.O1[cb + r] = acc1;
           a.O2[cb + r] = acc2;
+        } else if (MODE == COL_SHIFT) {
+          a.R1[cb + r] = acc1;
+          a.R2[cb + r] = acc2;
         } else {
           bufA[G.at(r)] = acc1;
           bufB[G.at(r)] = acc2;
@@ -200,6 +205,7 @@ __global__ void k_column(ColumnArgs a) {
       __syncwarp(gmask);
     }
   }
+  if (MODE == COL_SHIFT) return;
   const int nseq = MODE == COL_SOLVE ? 1 : (EXACT ? 4 : 0);
 #pragma unroll 1
   for (int k = (MODE == COL_SOLVE && EXACT) ? nseq : 0; k < nseq; ++k) {
@@ -505,8 +511,9 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
     }
     return cudaGetLastError();
   }
-  // the untiled and fused forms read FP64 product spectra only
-  if (MODE != COL_SOLVE && g.mp) return cudaErrorInvalidValue;
+  // the untiled and fused forms read FP64 product spectra only (the
+  // linear right-hand sides read none)
+  if (MODE != COL_SOLVE && MODE != COL_SHIFT && g.mp && NONLIN) return cudaErrorInvalidValue;
   if (MODE == COL_RHS) {  // one warp per column, four per block, no shared memory
     const int blocks = (g.ncol + 3) / 4;
     k_column<32, EXACT, NONLIN, COL_RHS><<<blocks, 128, 0, st>>>(a);
@@ -530,6 +537,10 @@ template <int P, bool EXACT, bool NONLIN>
 static cudaError_t launch_column_m(const ColumnArgs& a, int part, cudaStream_t st) {
   if (part == COL_RHS) return launch_column_t<P, EXACT, NONLIN, COL_RHS>(a, st);
   if (part == COL_SOLVE) return launch_column_t<P, EXACT, NONLIN, COL_SOLVE>(a, st);
+  if (part == COL_SHIFT) {
+    if constexpr (EXACT && !NONLIN) return launch_column_t<P, true, false, COL_SHIFT>(a, st);
+    return cudaErrorInvalidValue;
+  }
   return launch_column_t<P, EXACT, NONLIN, COL_FUSED>(a, st);
 }
 
@@ -564,6 +575,10 @@ cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysSca
   {
     const char* e = std::getenv("HST_RHS_TILED");
     a.tiled = !(e && std::atoi(e) == 0);
+  }
+  if (part == 4) {  // the right-hand-side stage, untiled (the per-piece prepare)
+    a.tiled = 0;
+    part = COL_RHS;
   }
   switch (g.P) {
     case 2: return launch_column_p<2>(a, exact, nonlin, part, st);

@@ -36,6 +36,42 @@ __device__ __forceinline__ ColConst col_const(int col, const Geometry& g, const 
   return c;
 }
 
+// The terms of product p (0..5: uu, vv, ww, uv, vw, uw) of buildrhs
+// (src/hst_equations.f90:167-209) from its D0, D1, D2 stencils q0, q1, q2,
+// added to the right-hand sides r1 (eta), r2 (d2v) with weight ode2 = ODE(2)
+// and to the carried terms o1, o2.
+__device__ __forceinline__ void product_rhs(int p, const ColConst& c, double ode2, cxd q0, cxd q1, cxd q2, cxd& r1,
+                                            cxd& r2, cxd& o1, cxd& o2) {
+  const double al = c.al, be = c.be, kk = c.kk;
+  cxd ru = mkc(0, 0), rw = mkc(0, 0), ex;
+  if (p == 0) {  // uu
+    ru = mkc(al * q0.y, -al * q0.x);
+    ex = cscale(-(al * al), q1);
+  } else if (p == 1) {  // vv
+    ex = cscale(kk, q1);
+  } else if (p == 2) {  // ww
+    rw = mkc(be * q0.y, -be * q0.x);
+    ex = cscale(-(be * be), q1);
+  } else if (p == 3) {  // uv
+    ru = cneg(q1);
+    ex = mkc(-al * q2.y + -(al * kk) * q0.y, al * q2.x + (al * kk) * q0.x);
+  } else if (p == 4) {  // vw
+    rw = cneg(q1);
+    ex = mkc(-be * q2.y + -(be * kk) * q0.y, be * q2.x + (be * kk) * q0.x);
+  } else {  // uw
+    ru = mkc(be * q0.y, -be * q0.x);
+    rw = mkc(al * q0.y, -al * q0.x);
+    ex = cscale(-((2.0 * al) * be), q1);
+  }
+  r2 = mkc(r2.x + ode2 * ex.x, r2.y + ode2 * ex.y);
+  o2 = cadd(o2, ex);
+  cxd e;
+  if (c.c00) e = mkc(ru.x, rw.x);
+  else e = mkc(-be * ru.y + al * rw.y, be * ru.x - al * rw.x);
+  r1 = mkc(r1.x + ode2 * e.x, r1.y + ode2 * e.y);
+  o1 = cadd(o1, e);
+}
+
 // TV(c, j): component c of V at row r + j - 2; TQ(p, j): product p at row
 // r + j - 2 (ghost phase applied); fsh(): the default-form shift factor of
 // row r, exp(-i (alfa dgx + beta dgz) y(r)), asked for last.  EXACT: no phase
@@ -115,33 +151,7 @@ __device__ __forceinline__ void rhs_point(const ColConst& c, const SubstepScalar
         a2 = QV{a2.x + e2 * qv.x, a2.y + e2 * qv.y};
       }
       const cxd q0 = mkc(a0.x, a0.y), q1 = mkc(a1.x, a1.y), q2 = mkc(a2.x, a2.y);
-      cxd ru = mkc(0, 0), rw = mkc(0, 0), ex;
-      if (p == 0) {  // uu
-        ru = mkc(al * q0.y, -al * q0.x);
-        ex = cscale(-(al * al), q1);
-      } else if (p == 1) {  // vv
-        ex = cscale(kk, q1);
-      } else if (p == 2) {  // ww
-        rw = mkc(be * q0.y, -be * q0.x);
-        ex = cscale(-(be * be), q1);
-      } else if (p == 3) {  // uv
-        ru = cneg(q1);
-        ex = mkc(-al * q2.y + -(al * kk) * q0.y, al * q2.x + (al * kk) * q0.x);
-      } else if (p == 4) {  // vw
-        rw = cneg(q1);
-        ex = mkc(-be * q2.y + -(be * kk) * q0.y, be * q2.x + (be * kk) * q0.x);
-      } else {  // uw
-        ru = mkc(be * q0.y, -be * q0.x);
-        rw = mkc(al * q0.y, -al * q0.x);
-        ex = cscale(-((2.0 * al) * be), q1);
-      }
-      r2 = mkc(r2.x + sc.ode1 * ex.x, r2.y + sc.ode1 * ex.y);
-      o2 = cadd(o2, ex);
-      cxd e;
-      if (c.c00) e = mkc(ru.x, rw.x);
-      else e = mkc(-be * ru.y + al * rw.y, be * ru.x - al * rw.x);
-      r1 = mkc(r1.x + sc.ode1 * e.x, r1.y + sc.ode1 * e.y);
-      o1 = cadd(o1, e);
+      product_rhs(p, c, sc.ode1, q0, q1, q2, r1, r2, o1, o2);
     }
   }
   if (c.masked) {  // damping_mask

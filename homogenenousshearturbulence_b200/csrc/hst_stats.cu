@@ -41,18 +41,25 @@ __device__ __forceinline__ void block_sums(double (&v)[NV], double* __restrict__
     }
 }
 
-// partials: eps (k^2 |u|^2), uv, uu, vv, ww, vw, uw, mfx, mfz
+// partials: eps (k^2 |u|^2), uv, uu, vv, ww, vw, uw, mfx, mfz, then q_out
+// (the weighted |u|^2 of every column but the mean), ed and pd (the energy in
+// the damped columns and its damping rate, gsoft = 1 for the soft damping);
+// the Stokes layer is not part of the GPU substep, so no row is inside it and
+// q_in, e_in are zero
+constexpr int ST_NM = 12;
 __global__ void __launch_bounds__(32 * ST_WARPS) k_stats_moments(Geometry g, PhysScalars ps,
                                                                  const double2* __restrict__ V1,
                                                                  const double2* __restrict__ V2,
                                                                  const double2* __restrict__ V3,
                                                                  const double* __restrict__ dyl,
+                                                                 const double* __restrict__ gdamp, double gsoft,
                                                                  double* __restrict__ partial) {
-  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double v[ST_NM] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int col = blockIdx.x * ST_WARPS + warp; col < g.ncol; col += gridDim.x * ST_WARPS) {
     const int ix = col / g.nzT, iz = col - ix * g.nzT - g.nz;
     const double al = ps.alfa0 * ix, be = ps.beta0 * iz, kk = al * al + be * be;
+    const double gd = gdamp[col];
     const size_t cb = (size_t)col * g.rows + 2;
     for (int iy = lane; iy < g.ny; iy += 32) {
       const cxd u = V1[cb + iy], vv = V2[cb + iy], w = V3[cb + iy];
@@ -60,6 +67,11 @@ __global__ void __launch_bounds__(32 * ST_WARPS) k_stats_moments(Geometry g, Phy
       if (ix == 0 && iz == 0) {
         v[7] += u.x * d;
         v[8] += w.x * d;
+        if (gd > 0.0) {
+          const double qc = d * ((u.x * u.x + u.y * u.y) + (w.x * w.x + w.y * w.y));
+          v[10] += qc;
+          v[11] += 2.0 * gsoft * gd * qc;
+        }
         v[2] += d * (u.x * u.x + u.y * u.y);
         v[4] += d * (w.x * w.x + w.y * w.y);
         v[6] += d * (u.x * w.x + u.y * w.y);
@@ -67,6 +79,11 @@ __global__ void __launch_bounds__(32 * ST_WARPS) k_stats_moments(Geometry g, Phy
       }
       const double wt = ix == 0 ? d : 2.0 * d;
       const double pu = u.x * u.x + u.y * u.y, pv = vv.x * vv.x + vv.y * vv.y, pw = w.x * w.x + w.y * w.y;
+      if (gd > 0.0) {
+        const double qc = wt * (pu + pv + pw);
+        v[10] += qc;
+        v[11] += 2.0 * gsoft * gd * qc;
+      }
       v[2] += wt * pu;
       v[3] += wt * pv;
       v[4] += wt * pw;
@@ -74,9 +91,32 @@ __global__ void __launch_bounds__(32 * ST_WARPS) k_stats_moments(Geometry g, Phy
       v[5] += wt * (w.x * vv.x + w.y * vv.y);
       v[6] += wt * (u.x * w.x + u.y * w.y);
       v[0] += wt * kk * (pu + pv + pw);
+      v[9] += wt * (pu + pv + pw);
     }
   }
-  block_sums<9>(v, partial);
+  block_sums<ST_NM>(v, partial);
+}
+
+// the column energies exz(iz, ix) = sum_y w |u|^2 (src/hst_stats.f90:225-240),
+// one warp per column, lanes over rows, a fixed order
+__global__ void __launch_bounds__(32 * ST_WARPS) k_stats_columns(Geometry g, const double2* __restrict__ V1,
+                                                                 const double2* __restrict__ V2,
+                                                                 const double2* __restrict__ V3,
+                                                                 const double* __restrict__ dyl,
+                                                                 double* __restrict__ exz) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int col = blockIdx.x * ST_WARPS + warp;
+  if (col >= g.ncol) return;
+  const int ix = col / g.nzT;
+  const size_t cb = (size_t)col * g.rows + 2;
+  double q = 0.0;
+  for (int iy = lane; iy < g.ny; iy += 32) {
+    const cxd u = V1[cb + iy], vv = V2[cb + iy], w = V3[cb + iy];
+    const double wt = ix == 0 ? dyl[iy] : 2.0 * dyl[iy];
+    q += wt * ((u.x * u.x + u.y * u.y) + (vv.x * vv.x + vv.y * vv.y) + (w.x * w.x + w.y * w.y));
+  }
+  for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+  if (lane == 0) exz[col] = q;
 }
 
 // the weighted sum of |q|^2 over every column (q: the DY solve of one component)
@@ -97,17 +137,29 @@ __global__ void __launch_bounds__(32 * ST_WARPS) k_stats_grad(Geometry g, const 
   block_sums<1>(v, partial);
 }
 
-// out: energy, dissipation, uv, vw, uu, vv, ww, uw (the order of the
-// Runtimedata columns the reference writes)
+// out[0..7]: energy, dissipation, uv, vw, uu, vv, ww, uw (the order of the
+// Runtimedata columns the reference writes); out[8..23]: the reference's
+// sums array before the box-mean correction (eps, uv, uu, vv, ww, vw, uw,
+// mfx, mfz, q_in, q_out, e_in, e_out, ed, pd; ncol_damped is the host's)
 __global__ void k_stats_final(int nblk, const double* __restrict__ pm, const double* __restrict__ pg, double ly_w,
                               double ni, double ly, double* __restrict__ out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double s[ST_NM] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int b = 0; b < nblk; ++b)
-    for (int k = 0; k < 9; ++k) s[k] += pm[(size_t)b * 9 + k];
+    for (int k = 0; k < ST_NM; ++k) s[k] += pm[(size_t)b * ST_NM + k];
   double eps = s[0];
   for (int c = 0; c < 3; ++c)
     for (int b = 0; b < nblk; ++b) eps += pg[(size_t)c * nblk + b];
+  double* raw = out + 8;
+  raw[0] = eps;
+  for (int k = 1; k < 9; ++k) raw[k] = s[k];
+  raw[9] = 0.0;    // q_in
+  raw[10] = s[9];  // q_out
+  raw[11] = 0.0;   // e_in
+  raw[12] = eps;   // e_out
+  raw[13] = s[10];
+  raw[14] = s[11];
+  raw[15] = 0.0;
   double uu = s[2] - s[7] * s[7] / ly_w, ww = s[4] - s[8] * s[8] / ly_w, uw = s[6] - s[7] * s[8] / ly_w;
   const double vv = s[3], uv = s[1], vw = s[5];
   const double inv = 1.0 / ly;
@@ -223,11 +275,19 @@ int stats_blocks(const Geometry& g, int nsm) {
   return b < need ? b : need;
 }
 
-cudaError_t launch_stats_moments(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double* partial,
-                                 cudaStream_t st) {
-  k_stats_moments<<<stats_blocks(g, d.nsm), 32 * ST_WARPS, 0, st>>>(g, ps, d.F[0], d.F[1], d.F[2], d.dyl, partial);
+cudaError_t launch_stats_moments(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double gsoft,
+                                 double* partial, cudaStream_t st) {
+  k_stats_moments<<<stats_blocks(g, d.nsm), 32 * ST_WARPS, 0, st>>>(g, ps, d.F[0], d.F[1], d.F[2], d.dyl, d.gdamp,
+                                                                     gsoft, partial);
   return cudaGetLastError();
 }
+
+cudaError_t launch_stats_columns(const Geometry& g, const DeviceState& d, double* exz, cudaStream_t st) {
+  k_stats_columns<<<(g.ncol + ST_WARPS - 1) / ST_WARPS, 32 * ST_WARPS, 0, st>>>(g, d.F[0], d.F[1], d.F[2], d.dyl, exz);
+  return cudaGetLastError();
+}
+
+int stats_partials() { return ST_NM; }
 
 cudaError_t launch_stats_grad(const Geometry& g, const DeviceState& d, int field, double* partial, cudaStream_t st) {
   k_stats_grad<<<stats_blocks(g, d.nsm), 32 * ST_WARPS, 0, st>>>(g, d.F[field], d.dyl, partial);

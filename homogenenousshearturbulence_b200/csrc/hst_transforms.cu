@@ -335,6 +335,83 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   }
 }
 
+// --------------------------------------- the reference-layout transforms ----
+// FFT, IFT, RFT and HFT (src/hst_fft.f90:181-237) on the buffers of the
+// per-piece path, which hold the reference's layouts: VVdz(nzd, nx+1,
+// -2:ny+1, 3) and VVdx / VVdp(nxd+1, nzd, -2:ny+1, 3), the latter also seen as
+// 2(nxd+1) reals a line (rVVdx, products).  A block loads LPB whole lines
+// into shared memory, transforms them there with the runtime plan and
+// writes them back over the same bytes (every line is read before any is
+// written, so the in-place real <-> complex layouts are safe).  These serve
+// the drop-in per-piece interface; the fused substep does not use them.
+static int fft_threads(int points, int ppt);
+struct PieceLines {
+  double2* base;  // line l starts at base + l * stride (complex elements)
+  size_t stride;
+  int kind;       // 0: complex z line; 1: c2r x line (Hermitian, nxd+1 modes in); 2: r2c x line (reals in)
+  int N;          // transform length
+};
+__device__ __forceinline__ double2 piece_load(const PieceLines& P, int l, int k) {
+  const double2* b = P.base + (size_t)l * P.stride;
+  if (P.kind == 0) return b[k];
+  if (P.kind == 1) {
+    const int h = P.N / 2;
+    if (k <= h) return b[k];
+    const double2 c = b[P.N - k];
+    return make_double2(c.x, -c.y);
+  }
+  const double* r = reinterpret_cast<const double*>(b);
+  return make_double2(r[k], 0.0);
+}
+template <int S>
+__global__ void __launch_bounds__(256) k_piece_lines(PieceLines P, int nlines, int lpb, const double2* __restrict__ tw) {
+  extern __shared__ double2 sh_d[];
+  const int N = P.N, LS = N + 1;
+  const int l0 = blockIdx.x * lpb;
+  const int nl = min(lpb, nlines - l0);
+  for (int e = threadIdx.x; e < lpb * N; e += blockDim.x) {
+    const int l = e / N, k = e - l * N;
+    sh_d[l * LS + k] = l < nl ? piece_load(P, l0 + l, k) : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const ShLinesT<double2> L = {sh_d, LS};
+  fft_global<S, 16, true, true>(N, lpb, tw, sh_d, L, L);
+  __syncthreads();
+  if (P.kind == 1) {  // real parts: 2(nxd+1) reals a line, the two past N zero
+    for (int e = threadIdx.x; e < nl * (N + 2); e += blockDim.x) {
+      const int l = e / (N + 2), k = e - l * (N + 2);
+      double* r = reinterpret_cast<double*>(P.base + (size_t)(l0 + l) * P.stride);
+      r[k] = k < N ? sh_d[l * LS + k].x : 0.0;
+    }
+  } else {
+    const int nout = P.kind == 0 ? N : N / 2 + 1;
+    for (int e = threadIdx.x; e < nl * nout; e += blockDim.x) {
+      const int l = e / nout, k = e - l * nout;
+      P.base[(size_t)(l0 + l) * P.stride + k] = sh_d[l * LS + k];
+    }
+  }
+}
+
+// kind 0/1/2 as PieceLines; S the transform's sign (+1 backward)
+cudaError_t launch_piece_lines(const DeviceState& d, double2* base, size_t stride, int nlines, int N, int kind, int S,
+                               const double2* tw, cudaStream_t st) {
+  if (!plan_ok(N) || nlines <= 0) return cudaErrorInvalidValue;
+  const PieceLines P = {base, stride, kind, N};
+  const int lpb = N >= 1536 ? 1 : (N >= 768 ? 2 : 4);
+  const int threads = fft_threads(lpb * N, 16);
+  if (threads > 256) return cudaErrorInvalidValue;
+  const size_t smem = (size_t)lpb * (N + 1) * sizeof(double2);
+  const int blocks = (nlines + lpb - 1) / lpb;
+  if (S > 0) {
+    smem_limit(d, k_piece_lines<+1>, 220 * 1024);
+    k_piece_lines<+1><<<blocks, threads, smem, st>>>(P, nlines, lpb, tw);
+  } else {
+    smem_limit(d, k_piece_lines<-1>, 220 * 1024);
+    k_piece_lines<-1><<<blocks, threads, smem, st>>>(P, nlines, lpb, tw);
+  }
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------- staged twiddles ----
 // The twiddles of the 8-point plan of N in stage order (see fft_stage_io):
 // for each stage after the first, [r - 1][kk] = W_N^(kk r N/(Ns R)).

@@ -25,6 +25,17 @@ LIB_PATH = PKG / "libhst_gpu.so"
 
 V1, V2, V3, OLD1, OLD2, RHS1, RHS2 = range(7)
 KIND_D2V, KIND_ETA, KIND_POISSON, KIND_D0, KIND_DY = 1, 2, 3, 4, 5
+# transform buffers of the per-piece path, FFT kinds, layout changes (include/hst_gpu.h)
+BUF_VVDZ, BUF_VVDX, BUF_VVDP = 0, 1, 2
+FFT_FFT, FFT_IFT, FFT_RFT, FFT_HFT = 1, 2, 3, 4
+Z_TO_X, X_TO_Z = 0, 1
+
+
+def id_buf(buf, m):
+    """the registry id of component m (1..3) of a transform buffer"""
+    return 8 + 3 * buf + m - 1
+
+
 # RK_rai (src/hst_params.f90:108-111), one row per substep
 RK_RAI = ((120.0 / 32.0, 2.0, 0.0), (120.0 / 8.0, 50.0 / 8.0, 34.0 / 8.0), (120.0 / 20.0, 90.0 / 20.0, 50.0 / 20.0))
 PI = 3.141592653589793
@@ -100,6 +111,30 @@ def lib():
             "hst_gpu_download_async": (i, [vp, i, vp]),
             "hst_gpu_wait_io": (i, [vp]),
             "hst_gpu_outstats": (i, [vp, d, P(d)]),
+            "hst_gpu_outstats_sums": (i, [vp, d, P(d), P(d)]),
+            "hst_gpu_fft": (i, [vp, i, i]),
+            "hst_gpu_transpose": (i, [vp, i, i]),
+            "hst_gpu_transform_to_physical": (i, [vp]),
+            "hst_gpu_build_products": (i, [vp, i]),
+            "hst_gpu_products_to_spectral": (i, [vp]),
+            "hst_gpu_vvdz_to_field": (i, [vp, i, i]),
+            "hst_gpu_buildrhs_prepare": (i, [vp, P(d), d, d]),
+            "hst_gpu_buildrhs": (i, [vp, P(d), i]),
+            "hst_gpu_damping_update": (i, [vp, d]),
+            "hst_gpu_damping_mask": (i, [vp]),
+            "hst_gpu_shear_shift": (i, [vp, d, d]),
+            "hst_gpu_linsolve": (i, [vp, d, d]),
+            "hst_gpu_buffer_upload": (i, [vp, i, i, vp]),
+            "hst_gpu_buffer_download": (i, [vp, i, i, vp]),
+            "hst_gpu_buffer_pointer": (i, [vp, i, P(vp), P(ct.c_size_t)]),
+            "hst_gpu_register_host": (i, [vp, vp, ct.c_size_t, i]),
+            "hst_gpu_unregister_host": (i, [vp, vp]),
+            "hst_gpu_host_id": (i, [vp, vp]),
+            "hst_gpu_upload_host": (i, [vp, vp]),
+            "hst_gpu_download_host": (i, [vp, vp]),
+            "hst_gpu_line_solve_host": (i, [vp, i, d, vp, vp, i, d, d, d]),
+            "hst_gpu_fill_ghosts_host": (i, [vp, vp, d, d]),
+            "hst_gpu_vvdz_to_field_host": (i, [vp, vp, i]),
             "hst_gpu_pressure": (i, [vp, d, i]),
             "hst_gpu_autotune": (i, [vp, d, i, ct.c_char_p, i]),
             "hst_gpu_write_restart": (i, [vp, ct.c_char_p, d, d, d, d, d]),
@@ -379,6 +414,132 @@ class Solver:
         self._check(lib().hst_gpu_outstats(self._h, t, out.ctypes.data_as(ct.POINTER(ct.c_double))), "outstats")
         return dict(zip(["energy", "diss", "uv", "vw", "uu", "vv", "ww", "uw"], out))
 
+    # ---- the substep one piece at a time (reference-layout buffers)
+    def buffer_shape(self, buf):
+        """numpy shape of one component of a buffer: VVdz(nzd, nx+1, rows) is
+        (rows, nx+1, nzd); VVdx, VVdp(nxd+1, nzd, rows) are (rows, nzd, nxd+1)
+        complex128 (2(nxd+1) reals along the last axis in their real view)"""
+        rows = self.ny + 4
+        return (rows, self.nx + 1, self.nzd) if buf == BUF_VVDZ else (rows, self.nzd, self.nxd + 1)
+
+    def buffer_download(self, buf, m) -> np.ndarray:
+        a = np.empty(self.buffer_shape(buf), np.complex128)
+        self._check(lib().hst_gpu_buffer_download(self._h, buf, m, a.ctypes.data), "buffer_download")
+        return a
+
+    def buffer_upload(self, buf, m, a):
+        a = np.ascontiguousarray(a, np.complex128)
+        if a.shape != self.buffer_shape(buf):
+            raise ValueError(f"buffer shape {a.shape}, expected {self.buffer_shape(buf)}")
+        self._check(lib().hst_gpu_buffer_upload(self._h, buf, m, a.ctypes.data), "buffer_upload")
+
+    def buffer_pointer(self, buf):
+        """(device address, bytes) of a whole buffer"""
+        ptr, n = ct.c_void_p(), ct.c_size_t()
+        self._check(lib().hst_gpu_buffer_pointer(self._h, buf, ct.byref(ptr), ct.byref(n)), "buffer_pointer")
+        return ptr.value, n.value
+
+    def fft(self, kind, m):
+        self._check(lib().hst_gpu_fft(self._h, kind, m), "fft")
+
+    def transpose(self, direction, m):
+        self._check(lib().hst_gpu_transpose(self._h, direction, m), "transpose")
+
+    def transform_to_physical(self):
+        self._check(lib().hst_gpu_transform_to_physical(self._h), "transform_to_physical")
+
+    def build_products(self, g):
+        self._check(lib().hst_gpu_build_products(self._h, int(g)), "build_products")
+
+    def products_to_spectral(self):
+        self._check(lib().hst_gpu_products_to_spectral(self._h), "products_to_spectral")
+
+    def vvdz_to_field(self, field, m):
+        self._check(lib().hst_gpu_vvdz_to_field(self._h, field, m), "vvdz_to_field")
+
+    def buildrhs_prepare(self, ode, deltat=None, time=None):
+        dt = self.deltat if deltat is None else float(deltat)
+        t = self.time if time is None else float(time)
+        o = (ct.c_double * 3)(*[float(x) for x in ode])
+        self._check(lib().hst_gpu_buildrhs_prepare(self._h, o, dt, t), "buildrhs_prepare")
+
+    def buildrhs(self, ode, g):
+        o = (ct.c_double * 3)(*[float(x) for x in ode])
+        self._check(lib().hst_gpu_buildrhs(self._h, o, int(g)), "buildrhs")
+
+    def damping_update(self, time=None):
+        t = self.time if time is None else float(time)
+        self._check(lib().hst_gpu_damping_update(self._h, t), "damping_update")
+
+    def damping_mask(self):
+        self._check(lib().hst_gpu_damping_mask(self._h), "damping_mask")
+
+    def shear_shift(self, dt_sub, time=None):
+        t = self.time if time is None else float(time)
+        self._check(lib().hst_gpu_shear_shift(self._h, float(dt_sub), t), "shear_shift")
+
+    def linsolve(self, lam, time=None):
+        t = self.time if time is None else float(time)
+        self._check(lib().hst_gpu_linsolve(self._h, float(lam), t), "linsolve")
+
+    def timestep_by_pieces(self, deltat=None, product_hook=None):
+        """timestep() (src/hst_equations.f90:56-87) called piece by piece, as
+        the reference's loop calls its module procedures; product_hook(g), if
+        given, runs between build_products(g) and products_to_spectral() (the
+        place tests/test_conservation.f90 edits the products).  Returns the
+        CFL number of the third substep."""
+        dt = self.deltat if deltat is None else float(deltat)
+        linear = bool(self.cfg.get("linear"))
+        cfl = 0.0
+        for i in range(3):
+            ode = RK_RAI[i]
+            if not linear or i == 2:
+                self.transform_to_physical()
+            if i == 2:
+                cfl = self.compute_cfl()
+            self.damping_update(self.time)
+            self.buildrhs_prepare(ode, dt, self.time)
+            if not linear:
+                for g in (1, 2):
+                    self.build_products(g)
+                    if product_hook is not None:
+                        product_hook(g)
+                    self.products_to_spectral()
+                    self.buildrhs(ode, g)
+            self.damping_mask()
+            dt_sub = 2.0 / ode[0] * dt
+            self.shear_shift(dt_sub, self.time)
+            self.time = self.time + dt_sub
+            self.linsolve(ode[0] / dt, self.time)
+        self.cfl = cfl
+        return cfl
+
+    # ---- host address registry (what a Fortran shim uses)
+    def register_host(self, addr: int, nbytes: int, ident: int):
+        self._check(lib().hst_gpu_register_host(self._h, ct.c_void_p(addr), nbytes, ident), "register_host")
+
+    def unregister_host(self, addr: int):
+        self._check(lib().hst_gpu_unregister_host(self._h, ct.c_void_p(addr)), "unregister_host")
+
+    def host_id(self, addr: int) -> int:
+        return int(lib().hst_gpu_host_id(self._h, ct.c_void_p(addr)))
+
+    SUM_NAMES = ("eps", "uv", "uu", "vv", "ww", "vw", "uw", "mfx", "mfz", "q_in", "q_out", "e_in", "e_out", "ed", "pd",
+                 "ncol_damped")
+
+    def outstats_sums(self, time=None):
+        """The reductions of outstats as the reference's `sums` array holds
+        them (src/hst_stats.f90:242; box-height integrals before the mean
+        correction) and the column energies exz as an (nx+1, 2nz+1) array
+        (exz[ix, iz + nz] = sum_y w |u|^2, :225-240).  RHS1 is overwritten."""
+        t = self.time if time is None else float(time)
+        sums = np.zeros(16)
+        exz = np.zeros((self.nx + 1, 2 * self.nz + 1))
+        P = ct.POINTER(ct.c_double)
+        self._check(lib().hst_gpu_outstats_sums(self._h, t, sums.ctypes.data_as(P), exz.ctypes.data_as(P)),
+                    "outstats_sums")
+        return dict(zip(self.SUM_NAMES, sums)), exz
+
     def autotune(self, deltat=None, steps: int = 3) -> str:
         """Pick the fastest line-solver group width and FFT plans for this
         context's sizes (the fields are left as they were); returns the report."""
@@ -426,6 +587,52 @@ class Solver:
     @property
     def stream(self) -> int:
         return int(lib().hst_gpu_stream(self._h) or 0)
+
+
+class ColumnSpectrum:
+    """The running average of the column energies that spectrum_write
+    (src/hst_stats.f90:110-134) keeps between its calls: add() every outstats
+    sample (the sums and exz of Solver.outstats_sums), energies() the
+    average E(ix, iz) = exz_acc / nacc / 2, the (0,0) column taken about the
+    box mean (the squared box means of the mean-flow profiles removed)."""
+
+    def __init__(self, dyl, t0=0.0):
+        self.ly_w = float(np.sum(dyl))
+        self.reset(t0)
+
+    def reset(self, t0=0.0):
+        self.acc = None
+        self.nacc = 0
+        self.mean_acc = 0.0
+        self.t0 = t0
+
+    def add(self, sums: dict, exz: np.ndarray):
+        self.acc = exz.copy() if self.acc is None else self.acc + exz
+        self.nacc += 1
+        self.mean_acc += (sums["mfx"] ** 2 + sums["mfz"] ** 2) / self.ly_w
+
+    def energies(self) -> np.ndarray:
+        """(nx+1, 2nz+1): 0.5 times the averaged column energies."""
+        if not self.nacc:
+            raise HstError("no samples")
+        full = self.acc / self.nacc
+        nz = (full.shape[1] - 1) // 2
+        full[0, nz] -= self.mean_acc / self.nacc
+        return 0.5 * full
+
+    def write(self, path, time, alfa0, beta0):
+        """The text file of spectrum_write: one line per column, ix, iz, kx,
+        kz, E; restarts the average."""
+        e = self.energies()
+        nx, nzT = e.shape
+        nz = (nzT - 1) // 2
+        with open(path, "w") as f:
+            f.write(f"# column energies ly/2 sum_y |u|^2 averaged over t = {self.t0:12.5f} .. {time:12.5f} "
+                    f"({self.nacc} samples);  ix  iz  kx  kz  E\n")
+            for ix in range(nx):
+                for iz in range(-nz, nz + 1):
+                    f.write(f"{ix:5d} {iz:5d} {alfa0 * ix:15.7E} {beta0 * iz:15.7E} {e[ix, iz + nz]:15.7E}\n")
+        self.reset(time)
 
 
 def device_bytes(**deck) -> float:

@@ -33,11 +33,13 @@
 #ifndef HST_GPU_H
 #define HST_GPU_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
 
-#define HST_GPU_ABI_VERSION 2
+#define HST_GPU_ABI_VERSION 3
 
 /* status classes */
 #define HST_OK 0
@@ -164,6 +166,16 @@ int hst_gpu_compute_cfl(hst_ctx* ctx, double* cfl);
  * averages, FP64, a fixed reduction order).  The dissipation's y part
  * comes from DY solves through HST_RHS1, which is overwritten. */
 int hst_gpu_outstats(hst_ctx* ctx, double time, double* out);
+/* The reductions of outstats as the reference leaves them in its `sums`
+ * array (src/hst_stats.f90:242), before the box-mean correction and the
+ * division by ly: sums[0..15] = eps, uv, uu, vv, ww, vw, uw, mfx, mfz, q_in,
+ * q_out, e_in, e_out, ed, pd, ncol_damped (box-height integrals, rows
+ * weighted by dyl; q_in and e_in are 0, as no row lies in a Stokes layer).
+ * exz (may be NULL): the column energies exz(-nz:nz, 0:nx) = sum_y w |u|^2
+ * of the 2-D spectrum (:225-240), (2nz+1)(nx+1) doubles, iz fastest, for the
+ * caller's running average (spectrum_write, :110-134).  RHS1 is
+ * overwritten. */
+int hst_gpu_outstats_sums(hst_ctx* ctx, double time, double* sums, double* exz);
 
 /* Tries the launch choices that keep every buffer's layout -- the lanes of
  * a line-solver group and the points a thread of the x and z FFT plans --
@@ -195,6 +207,98 @@ int hst_gpu_read_restart(hst_ctx* ctx, const char* path, double* time);
 
 /* device_sync() (src/hst_fft.f90:162) */
 int hst_gpu_sync(hst_ctx* ctx);
+
+/* ------------------------------------------ the substep one piece at a time */
+/* The module procedures a caller that runs the substep's pieces itself needs
+ * (the reference's test programs do, e.g. tests/test_conservation.f90:56-82,
+ * which edits the products between build_products and products_to_spectral).
+ * They work on the transform buffers of hst_fft in the reference's layouts
+ * (src/hst_fft.f90:39-46, 88-94), complex128, rows -2..ny+1 included:
+ *   HST_BUF_VVDZ  VVdz(nzd, nx+1, -2:ny+1, 3)
+ *   HST_BUF_VVDX  VVdx(nxd+1, nzd, -2:ny+1, 3), the same bytes as the reals
+ *                 rVVdx(2(nxd+1), nzd, -2:ny+1, 3)
+ *   HST_BUF_VVDP  VVdp(nxd+1, nzd, -2:ny+1, 3), the same bytes as the reals
+ *                 products(2(nxd+1), nzd, -2:ny+1, 3)
+ * The first call that needs them allocates the three buffers (at 768^2 x 512
+ * about 15 GB) and zeroes them.  The fused hst_gpu_timestep does not use
+ * them; its results agree with a substep run piece by piece to round-off.
+ * Component arguments m are 1..3 as in the Fortran. */
+#define HST_BUF_VVDZ 0
+#define HST_BUF_VVDX 1
+#define HST_BUF_VVDP 2
+/* FFT, IFT, RFT, HFT (src/hst_fft.f90:181-237): z forward and backward on
+ * VVdz(:,:,:,m) (complex, unnormalised); x complex-to-real VVdx(:,:,:,m) ->
+ * rVVdx(:,:,:,m) (the imaginary parts of kx = 0 and nxd ignored, as FFTW's
+ * c2r) and real-to-complex products(:,:,:,m) -> VVdp(:,:,:,m), in place */
+#define HST_FFT_FFT 1
+#define HST_FFT_IFT 2
+#define HST_FFT_RFT 3
+#define HST_FFT_HFT 4
+int hst_gpu_fft(hst_ctx* ctx, int kind, int m);
+/* the local layout changes of a one-rank run (src/hst_mpi.f90:751-784):
+ * HST_Z_TO_X  VVdz(:,:,:,m) -> VVdx(:,:,:,m), x modes above nx zeroed
+ *             (with zero_vvdx_padding, src/hst_transforms.f90:58-72)
+ * HST_X_TO_Z  VVdp(:,:,:,m) -> VVdz(:,:,:,m), the x modes 0..nx */
+#define HST_Z_TO_X 0
+#define HST_X_TO_Z 1
+int hst_gpu_transpose(hst_ctx* ctx, int dir, int m);
+/* transform_to_physical() (src/hst_transforms.f90:74-83): V -> rVVdx(:,:,:,1:3),
+ * every row */
+int hst_gpu_transform_to_physical(hst_ctx* ctx);
+/* build_products(g) (src/hst_transforms.f90:97-121), g = 1 (uu, vv, ww) or
+ * 2 (uv, vw, uw), times 1/(2 nxd nzd), into products(:,:,:,1:3) */
+int hst_gpu_build_products(hst_ctx* ctx, int g);
+/* products_to_spectral() (src/hst_transforms.f90:125-139): products -> VVdz */
+int hst_gpu_products_to_spectral(hst_ctx* ctx);
+/* vvdz_to_field(field, m) (src/hst_transforms.f90:143-160) into a field */
+int hst_gpu_vvdz_to_field(hst_ctx* ctx, int field, int m);
+/* buildrhs_prepare(ODE) (src/hst_equations.f90:92-141) with the module
+ * variables deltat and time passed: RHS1, RHS2, OLD1, OLD2 from V */
+int hst_gpu_buildrhs_prepare(hst_ctx* ctx, const double* ODE, double deltat, double time);
+/* buildrhs(ODE, g) (src/hst_equations.f90:151-213): the products of group g
+ * that VVdz holds, added to RHS1/2 and OLD1/2 */
+int hst_gpu_buildrhs(hst_ctx* ctx, const double* ODE, int g);
+/* damping_update(time) and damping_mask() (src/hst_damping.f90:80-133);
+ * no-ops when the deck has no (hard) damping */
+int hst_gpu_damping_update(hst_ctx* ctx, double time);
+int hst_gpu_damping_mask(hst_ctx* ctx);
+/* shear_shift(dt_sub) at `time` (src/hst_equations.f90:226-293): RHS1/2 and
+ * OLD1/2 to the frame of time + dt_sub; with exact_shift V1 (and V3) serve
+ * as scratch, as V(:,:,:,1) does in the reference (V is dead there) */
+int hst_gpu_shear_shift(hst_ctx* ctx, double dt_sub, double time);
+/* linsolve(lambda) at `time` (the time after the shift,
+ * src/hst_equations.f90:298-326): V from RHS1/2, every ghost row filled */
+int hst_gpu_linsolve(hst_ctx* ctx, double lambda, double time);
+/* one component of a buffer to / from the host (the reference layout) */
+int hst_gpu_buffer_upload(hst_ctx* ctx, int buf, int m, const double* host);
+int hst_gpu_buffer_download(hst_ctx* ctx, int buf, int m, double* host);
+/* the device address and bytes of a whole buffer (3 components), for a
+ * caller that works on it in place (on the context's stream) */
+int hst_gpu_buffer_pointer(hst_ctx* ctx, int buf, void** dptr, size_t* bytes);
+
+/* ------------------------------------------------ host address registry */
+/* The Fortran shim passes its arrays (V(:,:,:,c), rhs(:,:,:,k), VVdz(:,:,:,m),
+ * ...) by address; registering each array's base address once (from
+ * allocate_fields and init_fft, src/hst_setup.f90:42-71, src/hst_fft.f90:88-94)
+ * lets the calls below find the device copy, so the Fortran signatures stay
+ * as they are.  Ids: the field ids above, or HST_ID_BUF(buf, m) for one
+ * component of a buffer; `bytes` must be the size of that id.  No
+ * counterpart in the reference, whose arrays are mapped by OpenMP. */
+#define HST_ID_BUF(buf, m) (8 + 3 * (buf) + (m)-1)
+int hst_gpu_register_host(hst_ctx* ctx, const void* host, size_t bytes, int id);
+int hst_gpu_unregister_host(hst_ctx* ctx, const void* host);
+/* the id registered at this base address, or HST_EARG */
+int hst_gpu_host_id(const hst_ctx* ctx, const void* host);
+/* `!$omp target update to(a)` / `from(a)` of a registered array */
+int hst_gpu_upload_host(hst_ctx* ctx, const void* host);
+int hst_gpu_download_host(hst_ctx* ctx, void* host);
+/* line_solve, fill_ghosts_field and vvdz_to_field on registered fields,
+ * as the Fortran call sites pass them (src/hst_linsolve.f90:147-153,
+ * src/hst_derivatives.f90:149-157, src/hst_transforms.f90:143-160) */
+int hst_gpu_line_solve_host(hst_ctx* ctx, int sys, double lambda, const void* src, void* dst, int has_shift,
+                            double shift_x, double shift_z, double time);
+int hst_gpu_fill_ghosts_host(hst_ctx* ctx, void* field, double shift_x, double shift_z);
+int hst_gpu_vvdz_to_field_host(hst_ctx* ctx, void* field, int m);
 
 /* ------------------------------------------------------ host-side scalars */
 /* shear_shifts, s2_of, s2_integral (src/hst_derivatives.f90:85-128) for the

@@ -107,6 +107,7 @@ def lib():
             "ora_start": (None, [vp]),
             "ora_run": (ct.c_long, [vp, ct.c_long]),
             "ora_outstats": (None, [vp, P(d)]),
+            "ora_outstats_sums": (None, [vp, P(d), P(d)]),
             "ora_compute_pressure": (None, [vp, ct.c_int]),
             "ora_restart_write": (i, [vp, ct.c_char_p]),
             "ora_restart_read": (i, [vp, ct.c_char_p]),
@@ -308,6 +309,16 @@ class Sim:
 
     def run(self, max_steps):
         return lib().ora_run(self.h, int(max_steps))
+
+    def outstats_sums(self):
+        """outstats' 16 sums (eps, uv, uu, vv, ww, vw, uw, mfx, mfz, q_in,
+        q_out, e_in, e_out, ed, pd, ncol_damped) and the column energies
+        exz as an (nx+1, 2nz+1) array"""
+        sums = np.zeros(16)
+        exz = np.zeros((self.p.nx + 1, 2 * self.p.nz + 1))
+        lib().ora_outstats_sums(self.h, sums.ctypes.data_as(ct.POINTER(ct.c_double)),
+                                exz.ctypes.data_as(ct.POINTER(ct.c_double)))
+        return sums, exz
 
     def outstats(self):
         out = np.zeros(8)

@@ -162,6 +162,7 @@ struct ora_sim {
   std::vector<double> y, dyl, fy, der, k2, gdamp;
   std::vector<int> izd, inlayer;
   double theta_last;
+  int ncol_damped = 0;  // damped columns (src/hst_damping.f90:42)
   // fields
   long nf;
   std::vector<cx> F[7];  // V1 V2 V3 old1 old2 rhs1 rhs2
@@ -457,6 +458,7 @@ void ora_damping_update(ora_sim* s, double t) {
   if (theta == s->theta_last) return;
   s->theta_last = theta;
   double c = std::cos(theta), sn = std::sin(theta);
+  int n = 0;
   for (int ix = 0; ix <= s->nx; ++ix) {
     double kx = p.alfa0 * ix;
     for (int iz = -s->nz; iz <= s->nz; ++iz) {
@@ -475,8 +477,10 @@ void ora_damping_update(ora_sim* s, double t) {
       }
       if (ix == 0 && iz == 0 && !p.damp_mean) g = 0.0;
       s->gdamp[(size_t)(iz + s->nz) + (size_t)s->nzT * ix] = g;
+      if (g > 0.0) n = n + 1;
     }
   }
+  s->ncol_damped = n;
 }
 void ora_damping_mask(ora_sim* s) {
 #pragma omp parallel for
@@ -1288,6 +1292,115 @@ long ora_run(ora_sim* s, long max_steps) {
     new_timestep(s);
   }
   return n;
+}
+
+// The reductions of outstats (src/hst_stats.f90:136-243) as the reference
+// leaves them in its `sums` array before the box-mean correction:
+// sums = [eps, uv, uu, vv, ww, vw, uw, mfx, mfz, q_in, q_out, e_in, e_out,
+// ed, pd, ncol_damped] (box-height integrals over rows weighted by dyl), and
+// the column energies exz(-nz:nz, 0:nx) = sum_y w |u|^2 (:225-240).
+void ora_outstats_sums(ora_sim* s, double* sums, double* exz) {
+  const int nx = s->nx, nz = s->nz, ny = s->ny;
+  const int inc00 = stokes_active(s) ? 0 : 1;
+  const double gsoft = damping_soft_factor(s);
+  const int NV = 15;
+  std::vector<double> part((size_t)(nx + 1) * NV, 0.0);
+#pragma omp parallel for
+  for (int ix = 0; ix <= nx; ++ix) {
+    double v[15] = {0};  // eps uv uu vv ww vw uw mfx mfz q_in q_out e_in e_out ed pd
+    for (int iz = -nz; iz <= nz; ++iz) {
+      const size_t col = (size_t)(iz + nz) + (size_t)s->nzT * ix;
+      const double kk = s->k2[col], gd = s->gdamp[col];
+      for (int iy = 0; iy < ny; ++iy) {
+        cx cu = s->f(0, iy, iz, ix), cv = s->f(1, iy, iz, ix), cw = s->f(2, iy, iz, ix);
+        if (ix == 0 && iz == 0) {
+          v[7] = v[7] + cu.re * s->dyl[iy];
+          v[8] = v[8] + cw.re * s->dyl[iy];
+          if (gd > 0.0) {
+            double qc = s->dyl[iy] * (cu * conj(cu) + cw * conj(cw)).re;
+            v[13] = v[13] + qc;
+            v[14] = v[14] + 2.0 * gsoft * gd * qc;
+          }
+          if (inc00 == 1) {
+            v[2] = v[2] + s->dyl[iy] * (cu * conj(cu)).re;
+            v[4] = v[4] + s->dyl[iy] * (cw * conj(cw)).re;
+            v[6] = v[6] + s->dyl[iy] * (cu * conj(cw)).re;
+          }
+          continue;
+        }
+        double w = 2.0 * s->dyl[iy];
+        if (ix == 0) w = s->dyl[iy];
+        const double q = (cu * conj(cu) + cv * conj(cv) + cw * conj(cw)).re;
+        if (gd > 0.0) {
+          double qc = w * q;
+          v[13] = v[13] + qc;
+          v[14] = v[14] + 2.0 * gsoft * gd * qc;
+        }
+        v[2] = v[2] + w * (cu * conj(cu)).re;
+        v[3] = v[3] + w * (cv * conj(cv)).re;
+        v[4] = v[4] + w * (cw * conj(cw)).re;
+        v[1] = v[1] + w * (cu * conj(cv)).re;
+        v[5] = v[5] + w * (cw * conj(cv)).re;
+        v[6] = v[6] + w * (cu * conj(cw)).re;
+        v[0] = v[0] + w * kk * q;
+        if (s->inlayer[iy] == 1) {
+          v[9] = v[9] + w * q;
+          v[11] = v[11] + w * kk * q;
+        } else {
+          v[10] = v[10] + w * q;
+          v[12] = v[12] + w * kk * q;
+        }
+      }
+    }
+    for (int k = 0; k < NV; ++k) part[(size_t)ix * NV + k] = v[k];
+  }
+  for (int k = 0; k < 16; ++k) sums[k] = 0.0;
+  for (int ix = 0; ix <= nx; ++ix)
+    for (int k = 0; k < NV; ++k) sums[k] += part[(size_t)ix * NV + k];
+  // y derivatives of the three components into rhs1 (:198-223)
+  for (int c = 0; c < 3; ++c) {
+    ora_line_solve(s, ORA_DY, 0.0, c, ORA_RHS1, 0, 0, 0);
+    std::vector<double> gp((size_t)(nx + 1) * 3, 0.0);
+#pragma omp parallel for
+    for (int ix = 0; ix <= nx; ++ix) {
+      double grad = 0, g_in = 0, g_out = 0;
+      for (int iz = -nz; iz <= nz; ++iz)
+        for (int iy = 0; iy < ny; ++iy) {
+          if (ix == 0 && iz == 0 && inc00 == 0) continue;
+          double w = 2.0 * s->dyl[iy];
+          if (ix == 0) w = s->dyl[iy];
+          cx dq = s->f(ORA_RHS1, iy, iz, ix);
+          const double q = (dq * conj(dq)).re;
+          grad = grad + w * q;
+          if (s->inlayer[iy] == 1) g_in = g_in + w * q;
+          else g_out = g_out + w * q;
+        }
+      gp[(size_t)ix * 3] = grad;
+      gp[(size_t)ix * 3 + 1] = g_in;
+      gp[(size_t)ix * 3 + 2] = g_out;
+    }
+    for (int ix = 0; ix <= nx; ++ix) {
+      sums[0] += gp[(size_t)ix * 3];
+      sums[11] += gp[(size_t)ix * 3 + 1];
+      sums[12] += gp[(size_t)ix * 3 + 2];
+    }
+  }
+  sums[15] = (double)(ora_damping_active(s) ? s->ncol_damped : 0);
+  // column energies
+  if (exz) {
+#pragma omp parallel for
+    for (int ix = 0; ix <= nx; ++ix)
+      for (int iz = -nz; iz <= nz; ++iz) {
+        double qc = 0.0;
+        for (int iy = 0; iy < ny; ++iy) {
+          cx cu = s->f(0, iy, iz, ix), cv = s->f(1, iy, iz, ix), cw = s->f(2, iy, iz, ix);
+          double w = 2.0 * s->dyl[iy];
+          if (ix == 0) w = s->dyl[iy];
+          qc = qc + w * (cu * conj(cu) + cv * conj(cv) + cw * conj(cw)).re;
+        }
+        exz[(size_t)(iz + nz) + (size_t)s->nzT * ix] = qc;
+      }
+  }
 }
 
 // outstats: src/hst_stats.f90:136-285 (energy, dissipation, uv, vw, normal stresses)

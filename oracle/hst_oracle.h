@@ -115,6 +115,9 @@ long ora_run(ora_sim* s, long max_steps);
 /* statistics of src/hst_stats.f90:136-285: out = energy, diss, uv, vw, uu, vv, ww, uw
  * (box means, Runtimedata columns 10-13 and variances_runtime.dat) */
 void ora_outstats(ora_sim* s, double* out);
+/* outstats' 16 reduction sums before the mean correction and the column
+ * energies exz(-nz:nz, 0:nx) (may be NULL) */
+void ora_outstats_sums(ora_sim* s, double* sums, double* exz);
 /* compute_pressure (src/hst_pressure.f90:35-110) into field dst; rhs1 is scratch */
 void ora_compute_pressure(ora_sim* s, int dst);
 

@@ -488,6 +488,43 @@ def test_outstats_matches_oracle(deck_over):
     s.close()
 
 
+DAMPED_DECKS = [dict(), dict(damp_kpar=3.0, damp_kperp=2.0, damp_rate=0.5, damp_edge=0.3),
+                dict(damp_kpar=3.0, damp_kperp=2.0, damp_hard=True, damp_mean=True),
+                dict(nx=63, nz=64, ny=32, exact_shift=True, s2_amplitude=0.5, s2_period=10.0, damp_kpar=4.0,
+                     damp_kperp=3.0, damp_rate=1.0, damp_edge=0.5, damp_mean=True)]
+
+
+@pytest.mark.parametrize("deck_over", DAMPED_DECKS)
+def test_outstats_sums_match_oracle(deck_over):
+    """hst_gpu_outstats_sums against the oracle's restatement of the
+    reference's sums (src/hst_stats.f90:136-243) after 30 substeps, with and
+    without large-scale damping: every sum within 1e-10 of the largest
+    magnitude among them, ncol_damped exactly, and the column energies exz
+    within 1e-10 of their maximum; two calls give identical numbers."""
+    deck = c1_deck(**deck_over)
+    V0 = seeded_field(deck, seed=6, k0=4.0, energy=0.1)
+    s, o = make_pair(deck, V0)
+    run_pair(s, o, deck["deltat"], 10)
+    g1, e1 = s.outstats_sums()
+    g2, e2 = s.outstats_sums()
+    r, er = o.outstats_sums()
+    assert g1 == g2 and np.array_equal(e1, e2)
+    names = hst.Solver.SUM_NAMES
+    scale = max(abs(v) for v in r[:15])
+    for k, name in enumerate(names[:15]):
+        assert abs(g1[name] - r[k]) <= 1e-10 * scale, (name, g1[name], r[k])
+    assert g1["ncol_damped"] == r[15]
+    if deck_over:
+        assert r[15] > 0 and r[13] > 0
+    assert np.abs(e1 - er).max() <= 1e-10 * np.abs(er).max()
+    # the box averages of outstats follow from the sums
+    st = s.outstats()
+    ly_w = float(np.sum(s.dyl))
+    q2 = (g1["uu"] - g1["mfx"] ** 2 / ly_w) + g1["vv"] + (g1["ww"] - g1["mfz"] ** 2 / ly_w)
+    assert abs(st["energy"] - 0.5 * q2 / deck["ly"]) <= 1e-12 * st["energy"]
+    s.close()
+
+
 # ------------------------------------------------------------ restart files ----
 def test_restart_files(golden, tmp_path):
     """hst_gpu_write_restart / hst_gpu_read_restart (src/hst_io.f90:69-178,
