@@ -66,7 +66,7 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def alg_bytes(deck, nxd, nzd, split, mixed=False):
+def alg_bytes(deck, nxd, nzd, split, mixed=False, shift_split=False):
     """Compulsory HBM bytes per launch of each kernel and per substep.
     Ns = ny (2nz+1)(nx+1) spectral points per component, Nzx = ny nzd (nx+1).
     With the column stage split, `rhs` streams V, Q, old in and old, rhs out
@@ -84,7 +84,10 @@ def alg_bytes(deck, nxd, nzd, split, mixed=False):
         "xprod": t * (3 * Nzx + 6 * Nzx),
         "zfwd": t * (6 * Nzx + 6 * Ns),
         "rhs": b * 9 * Ns + t * 6 * Ns,
-        "column": b * ((9 if deck.get("exact_shift") else 5) * Ns if split else 10 * Ns) + (0 if split else t * 6 * Ns),
+        "column": b * ((9 if deck.get("exact_shift") and not shift_split else 5) * Ns if split else 10 * Ns)
+                  + (0 if split else t * 6 * Ns),
+        # the exact_shift shift as a kernel of its own: rhs and old in and out
+        "shift": b * 8 * Ns,
     }
     sub = b * 13 * Ns + t * (12 * Ns + 18 * Nzx)
     return k, sub, Ns, Nzx
@@ -379,7 +382,8 @@ def roofline(deck, s, kt, mixed, sub_ms, config):
     """The top kernel's roofline (its algorithmic bytes per launch over its
     average launch time, against the measured HBM copy bandwidth) and the
     whole substep's (B_alg over the substep time)."""
-    per_kernel, b_sub, Ns, Nzx = alg_bytes(deck, s.nxd, s.nzd, kt.get("rhs", (0, 0))[1] > 0, mixed)
+    per_kernel, b_sub, Ns, Nzx = alg_bytes(deck, s.nxd, s.nzd, kt.get("rhs", (0, 0))[1] > 0, mixed,
+                                           kt.get("shift", (0, 0))[1] > 0)
     peak, peak_kind = peaks()
     top = max(kt, key=lambda k: kt[k][0])
     avg_ms = kt[top][0] / kt[top][1]

@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <unordered_set>
 #include <vector>
 
@@ -144,11 +145,15 @@ struct hst_ctx {
   unsigned long long* h_cfl;      // pinned CFL read-back
   std::string err;
   std::unordered_set<const void*> configured;  // kernels whose shared-memory limit is raised
+  std::unordered_map<uint64_t, int> occupancy;  // resident blocks an SM, per launch shape
   long long launches;
   int device;
   // the column stage as two kernels (right-hand sides streamed row by row,
   // then the solves) or one; HST_COLUMN_FUSED=1 selects the single kernel
   bool column_split;
+  // with exact_shift, the shift as a third kernel before the solves
+  // (HST_SHIFT_SPLIT=1)
+  bool shift_split;
   // per-kernel-class CUDA-event accounting (hst_gpu_set_profiling)
   bool prof_on;
   std::vector<cudaEvent_t> ev;
@@ -300,6 +305,7 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
     why = "ny must be even";
     return HST_EARG;
   }
+  g.edge_gap = 0;
   g.nxB = p.nx + 1;
   g.nzT = 2 * p.nz + 1;
   g.rows = p.ny + 4;
@@ -415,12 +421,56 @@ static void free_device(hst_ctx* c) {
   DeviceState& d = c->d;
   for (int i = 0; i < 7; ++i)
     if (d.F[i]) cudaFree(d.F[i]);
-  void* ps[] = {d.Z,    d.Pp,  d.Q,    d.der,   d.derS, d.d0tab, d.y,    d.dyl,  d.gdamp,
-                d.twx,  d.twz, d.twxf, d.twzf,  d.cfl,  d.stats, d.vvdz, d.vvdx, d.vvdp};
+  void* ps[] = {d.Z,    d.Pp,   d.Q,    d.der,  d.derS,  d.d0tab, d.y,    d.dyl,  d.gdamp, d.twx, d.twz,
+                d.twxf, d.twzf, d.cfl,  d.stats, d.vvdz, d.vvdx,  d.vvdp, d.Zg,   d.Ppg,  d.Qg};
   for (void* q : ps)
     if (q) cudaFree(q);
+  if (d.facg) cudaFree(d.facg);
   std::memset(&d, 0, sizeof d);
   d.configured = &c->configured;
+  d.occupancy = &c->occupancy;
+}
+
+// The column kernels' factor scratch in global memory: one slice of
+// (m-2) x 4 x P doubles per solver group that can be resident at once (at
+// most 16 warps an SM), sized for the current group width.  It is used (and
+// with it the persistent solve stage, k_column_solve) for slabs of 16 rows
+// or more, where the scratch would otherwise take half a warp's shared memory
+// (768^2 x 512: column 10.2 against 11.1 ms); at 8 rows a lane the one-column
+// kernel with the scratch in shared memory measured faster (384^2 x 256:
+// 0.54 against 0.75 ms).  HST_COLUMN_GFAC=1 / 0 forces either.
+static cudaError_t ensure_facg(hst_ctx* ctx) {
+  const Geometry& g = ctx->g;
+  const char* e = std::getenv("HST_COLUMN_GFAC");
+  const bool want = e ? std::atoi(e) == 1 : g.m >= 16;
+  if (!want) {
+    if (ctx->d.facg) {
+      cudaError_t r = cudaStreamSynchronize(ctx->stream);
+      if (r != cudaSuccess) return r;
+      cudaFree(ctx->d.facg);
+      ctx->d.facg = nullptr;
+      ctx->d.facg_doubles = 0;
+    }
+    return cudaSuccess;
+  }
+  const int nsm = ctx->d.nsm > 0 ? ctx->d.nsm : 148;
+  const size_t need = (size_t)nsm * 16 * (32 / std::min(g.P, 32)) * hst::column_fac_doubles(g);
+  if (ctx->d.facg && ctx->d.facg_doubles >= need) return cudaSuccess;
+  if (ctx->d.facg) {
+    cudaError_t r = cudaStreamSynchronize(ctx->stream);
+    if (r != cudaSuccess) return r;
+    cudaFree(ctx->d.facg);
+    ctx->d.facg = nullptr;
+    ctx->d.facg_doubles = 0;
+  }
+  cudaError_t r = cudaMalloc((void**)&ctx->d.facg, need * sizeof(double));
+  if (r != cudaSuccess) {
+    cudaGetLastError();
+    ctx->d.facg = nullptr;  // fall back to the scratch in shared memory
+    return cudaSuccess;
+  }
+  ctx->d.facg_doubles = need;
+  return cudaSuccess;
 }
 
 extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
@@ -433,6 +483,8 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   {
     const char* e = std::getenv("HST_COLUMN_FUSED");
     ctx->column_split = !(e && std::atoi(e) == 1);
+    const char* f = std::getenv("HST_SHIFT_SPLIT");
+    ctx->shift_split = f && std::atoi(f) == 1;
   }
   ctx->prof_on = false;
   for (int k = 0; k < HST_KC_N; ++k) {
@@ -444,6 +496,7 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   ctx->h_cfl = nullptr;
   std::memset(&ctx->d, 0, sizeof ctx->d);
   ctx->d.configured = &ctx->configured;
+  ctx->d.occupancy = &ctx->occupancy;
   std::string why;
   int rc = choose_geometry(*pin, ctx->g, why);
   if (rc != HST_OK) {
@@ -509,6 +562,11 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   ok = ok && alloc((void**)&d.Z, es * 3 * (size_t)g.nzd * g.ny * g.nxB);
   ok = ok && alloc((void**)&d.Pp, es * 6 * (size_t)g.nzd * g.ny * g.nxB);
   ok = ok && alloc((void**)&d.Q, es * 6 * (size_t)g.ncol * g.ny);
+  if (hst::edge_rows_needed(g, p.s2_amplitude != 0.0 || p.s2_mean != 0.0)) {
+    ok = ok && alloc((void**)&d.Zg, es * 3 * (size_t)g.nzd * g.nxB * 4);
+    ok = ok && alloc((void**)&d.Ppg, es * 6 * (size_t)g.nzd * g.nxB * 4);
+    ok = ok && alloc((void**)&d.Qg, es * 6 * (size_t)g.ncol * 4);
+  }
   ok = ok && alloc((void**)&d.der, sizeof(double) * 20 * (size_t)ny);
   ok = ok && alloc((void**)&d.derS, sizeof(double) * 20 * (size_t)ny);
   ok = ok && alloc((void**)&d.d0tab, sizeof(double) * hst::d0_table_doubles(ny));
@@ -572,6 +630,7 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   cudaError_t e = etab;
   if (e == cudaSuccess) e = hst::set_fft_constants();
   if (e == cudaSuccess) e = hst::make_transform_maps(g, d);
+  if (e == cudaSuccess) e = ensure_facg(ctx);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -963,6 +1022,7 @@ extern "C" int hst_gpu_autotune(hst_ctx* ctx, double deltat, int steps, char* re
     cudaError_t e = cudaMemcpy(ctx->d.derS, ds.data(), sizeof(double) * 20 * g.ny, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = hst::launch_d0_table(g, ctx->d, ctx->stream);
     if (e == cudaSuccess) e = hst::make_transform_maps(g, ctx->d);
+    if (e == cudaSuccess) e = ensure_facg(ctx);
     return e;
   };
   for (int P : lanes)
@@ -1158,8 +1218,18 @@ static int queue_timestep(hst_ctx* ctx, double* time, double deltat) {
     if (ctx->column_split) {
       CK(timed(ctx, HST_KC_RHS,
                [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, 1, ctx->stream); }));
-      CK(timed(ctx, HST_KC_COLUMN,
-               [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, 2, ctx->stream); }));
+      if (p.exact_shift && ctx->shift_split) {
+        // the exact_shift shift as a kernel of its own (two lines a group,
+        // no factor scratch: more warps an SM), then the solves
+        CK(timed(ctx, HST_KC_SHIFT,
+                 [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, 1, 0, 3, ctx->stream); }));
+        CK(timed(ctx, HST_KC_COLUMN,
+                 [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, 0, !p.linear, 2, ctx->stream); }));
+      } else {
+        CK(timed(ctx, HST_KC_COLUMN, [&] {
+          return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, 2, ctx->stream);
+        }));
+      }
     } else {
       CK(timed(ctx, HST_KC_COLUMN,
                [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, 0, ctx->stream); }));

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <unordered_map>
 #include <unordered_set>
 
 #include "../../include/hst_gpu.h"
@@ -22,6 +23,9 @@ struct Geometry {
   int Ty;              // y tile of the transforms (divides ny)
   int pptx, pptz;      // FFT points per thread of the x and z transforms (8: the low-register plans)
   int mp;              // mixed precision: Z, Pp, Q and their transforms in FP32 (complex64)
+  // 0, or (in the view of the four ghost rows that the edge transforms take)
+  // ny: the z-inverse then reads rows -2, -1, ny, ny+1 of V
+  int edge_gap;
 };
 
 struct DeviceState {
@@ -45,6 +49,12 @@ struct DeviceState {
   // (set by make_transform_maps when the x kernel's 8-point plan uses them)
   CUtensorMap tmZ, tmPp;
   bool maps;
+  // The products of the four ghost rows (-2, -1, ny, ny+1) transformed like
+  // the interior ones (null when their shear-periodic images are exact):
+  // Zg [3][nzd][nxB][4], Ppg [6][nzd][nxB][4], Qg [6][ncol][4], in the
+  // transforms' precision, with their TMA maps
+  double2 *Zg, *Ppg, *Qg;
+  CUtensorMap tmZg, tmPpg;
   int nsm;        // SMs of the device
   double* stats;  // outstats scratch: block partials of the moments (stats_partials() a block),
                   // of the three gradients (one a block each), then the 24 results
@@ -54,7 +64,32 @@ struct DeviceState {
   // kernels whose shared-memory limit has been raised in this context
   // (owned by the context; null: raise it at every launch)
   std::unordered_set<const void*>* configured;
+  // resident blocks an SM of (kernel, threads, shared bytes) launches, asked
+  // once (owned by the context; null: asked at every launch)
+  std::unordered_map<uint64_t, int>* occupancy;
+  // the column kernels' factor scratch in global memory (one slice per
+  // resident solver group; null: the scratch stays in shared memory)
+  double* facg;
+  size_t facg_doubles;
 };
+
+// Resident blocks an SM of kernel k with T threads and `smem` dynamic
+// shared bytes (cudaOccupancyMaxActiveBlocksPerMultiprocessor, cached).
+template <typename K>
+inline int blocks_per_sm(const DeviceState& d, K k, int T, size_t smem) {
+  const uint64_t key = (uint64_t)(uintptr_t)reinterpret_cast<const void*>(k) * 1000003ull ^ ((uint64_t)T << 40) ^ smem;
+  if (d.occupancy) {
+    auto it = d.occupancy->find(key);
+    if (it != d.occupancy->end()) return it->second;
+  }
+  int n = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, T, smem) != cudaSuccess || n < 1) {
+    cudaGetLastError();
+    n = 1;
+  }
+  if (d.occupancy) (*d.occupancy)[key] = n;
+  return n;
+}
 
 // Raises kernel k's dynamic shared-memory limit to `bytes`, once per context
 // (the attribute belongs to the function in the current context; setting it
@@ -99,6 +134,9 @@ cudaError_t launch_line_solve(const Geometry& g, const DeviceState& d, const Phy
 cudaError_t launch_fill_ghosts(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int field, double sx,
                                double sz, cudaStream_t st);
 size_t column_smem_bytes(const Geometry& g, int exact);
+// the two line buffers of a solver group, and its factor scratch (doubles)
+size_t column_lines_bytes(const Geometry& g);
+size_t column_fac_doubles(const Geometry& g);
 // the factored D0 matrix of the line-solve group (P, m of g) into d.d0tab,
 // from d.derS; d0_table_doubles: the table's size for any group of ny rows
 cudaError_t launch_d0_table(const Geometry& g, const DeviceState& d, cudaStream_t st);
@@ -135,6 +173,11 @@ cudaError_t launch_buildrhs_group(const Geometry& g, const DeviceState& d, const
 cudaError_t launch_damping_mask(const Geometry& g, const DeviceState& d, cudaStream_t st);
 cudaError_t launch_shift_default(const Geometry& g, const DeviceState& d, const PhysScalars& ps, double dgx,
                                  double dgz, cudaStream_t st);
+// the ghost rows' products must be transformed themselves (not taken as the
+// shear-periodic images of the interior rows): with a spanwise shift (S2) and
+// nzd = 3 nz, the retained modes iz = +-nz alias product modes -+2nz, whose
+// wrap phases differ
+bool edge_rows_needed(const Geometry& g, bool s2_active);
 // the TMA maps of Z and Pp for the x kernel (d.maps false when not used)
 cudaError_t make_transform_maps(const Geometry& g, DeviceState& d);
 // the stage-ordered twiddles of the 8-point plan of N into out (at most N

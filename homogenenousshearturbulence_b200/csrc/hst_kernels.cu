@@ -16,6 +16,7 @@
 // interior ones: the 3/2 rule makes the retained product modes exact, so the
 // image of row k is row k times the wrap phase, which the right-hand-side
 // stage applies when it reads them.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 
@@ -32,6 +33,7 @@ struct ColumnArgs {
   SubstepScalars sc;
   double2 *V1, *V2, *V3, *O1, *O2, *R1, *R2;
   const double2* Q;
+  const double2* Qg;  // the ghost rows' product spectra [6][ncol][4] (null: their wrap images)
   const double* der;
   const double* derS;
   const double* d0tab;
@@ -40,6 +42,8 @@ struct ColumnArgs {
   int* err;   // set to 1 by a kernel whose bounded wait ran out
   int tiled;  // the right-hand sides through k_rhs_tiled
   const DeviceState* dstate;  // host side only: the launch's context state
+  double* facg;               // global factor scratch of the persistent form (null: shared memory)
+  int fac_groups;             // groups that scratch holds
 };
 
 __device__ __forceinline__ unsigned group_mask(int P) {
@@ -48,10 +52,12 @@ __device__ __forceinline__ unsigned group_mask(int P) {
   return ((1u << P) - 1u) << ((lane / P) * P);
 }
 
-// a product spectrum at row q of its column, with the ghost images
-__device__ __forceinline__ cxd q_at(const double2* __restrict__ Qc, int q, int ny, cxd ph) {
-  if (q < 0) return cmul(Qc[q + ny], cconj(ph));
-  if (q >= ny) return cmul(Qc[q - ny], ph);
+// a product spectrum at row q of its column, with the ghost images (or,
+// with Qgc, the ghost rows' own transforms: rows -2, -1, ny, ny+1 there)
+__device__ __forceinline__ cxd q_at(const double2* __restrict__ Qc, const double2* __restrict__ Qgc, int q, int ny,
+                                    cxd ph) {
+  if (q < 0) return Qgc ? Qgc[q + 2] : cmul(Qc[q + ny], cconj(ph));
+  if (q >= ny) return Qgc ? Qgc[q - ny + 2] : cmul(Qc[q - ny], ph);
   return Qc[q];
 }
 
@@ -77,9 +83,13 @@ __device__ __forceinline__ void store_with_ghosts(double2* __restrict__ col, con
 // place and nothing else (the per-piece shear_shift).
 enum { COL_FUSED = 0, COL_RHS = 1, COL_SOLVE = 2, COL_SHIFT = 3 };
 
+// The work on one Fourier column (the body of k_column): bufA, bufB (bufC)
+// the group's line buffers in shared memory, fac its factor scratch (the
+// back-substitution factors of the D2V and ETA solves, (m-2) x 4 x P
+// doubles, in shared or in global memory).
 template <int P, bool EXACT, bool NONLIN, int MODE>
-__global__ void k_column(ColumnArgs a) {
-  extern __shared__ double smem_d[];
+__device__ __forceinline__ void column_body(const ColumnArgs& a, int col, int s, cxd* bufA, cxd* bufB, cxd* bufC,
+                                            double* fac) {
   const Geometry& g = a.g;
   const int ny = g.ny, nz = g.nz, nzT = g.nzT;
   LineGeom G;
@@ -88,21 +98,7 @@ __global__ void k_column(ColumnArgs a) {
   G.MS = g.MS;
   G.P = P;
   G.invm = (unsigned)((1u << 20) + g.m - 1) / (unsigned)g.m;
-  const int groups = blockDim.x / P;
-  const int grp = threadIdx.x / P, s = threadIdx.x - grp * P;
-  const int col = blockIdx.x * groups + grp;
-  if (col >= g.ncol) return;
   const unsigned gmask = group_mask(P);
-  const int mi = g.m - 2;
-  const int lineN = P * g.MS;
-  constexpr int NL = (EXACT && MODE == COL_FUSED) ? 3 : 2;  // lines held
-  const size_t per_group = (size_t)NL * lineN * 2 + (size_t)mi * 4 * P;  // doubles
-  double* base = smem_d + per_group * grp;
-  cxd* bufA = reinterpret_cast<cxd*>(base);
-  cxd* bufB = bufA + lineN;
-  cxd* bufC = bufB + lineN;  // EXACT and COL_FUSED only
-  double* fac = base + (size_t)NL * lineN * 2;
-
   const int ix = col / nzT, iz = col - ix * nzT - nz;
   const bool c00 = (ix == 0 && iz == 0);
   const double al = a.ps.alfa0 * ix, be = a.ps.beta0 * iz;
@@ -124,7 +120,9 @@ __global__ void k_column(ColumnArgs a) {
 #pragma unroll 1
     for (int r = s; r < ny; r += P) {
       auto tv = [&](int c, int j) -> cxd { return (c == 0 ? V1c : (c == 1 ? V2c : V3c))[r + j - 2]; };
-      auto tq = [&](int p, int j) -> cxd { return q_at(Qc + p * qs, r + j - 2, ny, cc.ph_t); };
+      auto tq = [&](int p, int j) -> cxd {
+        return q_at(Qc + p * qs, a.Qg ? a.Qg + ((size_t)p * g.ncol + col) * 4 : nullptr, r + j - 2, ny, cc.ph_t);
+      };
       const size_t ro = cb + r;
       cxd r1, r2, o1, o2;
       const double yr = a.y[r + 2];
@@ -298,6 +296,218 @@ __global__ void k_column(ColumnArgs a) {
   store_with_ghosts<P>(a.V3 + (size_t)col * g.rows, bufB, G, ny, phn, s, false);
 }
 
+// The five-point stencil n (0: D0, 1: D1) of a line held slab by slab in
+// shared memory, in place: lane s computes rows s m .. s m + m - 1 of its
+// slab with a sliding window, the two rows beyond each end of the slab from
+// the neighbouring lanes (by shuffle, taken before anything is written) and,
+// across the box edge, the shear-periodic ghost images f(ny + k) = f(k) ph,
+// f(-k) = f(ny - k) conj(ph) (wrap_rows, src/hst_mpi.f90:340-355).  The sum
+// runs over j = -2..2 in order, as the reference's stencils do.
+template <int P>
+__device__ __forceinline__ void slab_stencil(int n, const SlabDer& DS, cxd* sb, int m, int s, cxd ph, unsigned gmask) {
+  const cxd f0 = sb[0], f1 = sb[1], l0 = sb[m - 2], l1 = sb[m - 1];
+  const int up = (s + 1) & (P - 1), dn = (s - 1) & (P - 1);
+  cxd a0 = shfl_c(gmask, f0, up, P), a1 = shfl_c(gmask, f1, up, P);  // rows s m + m, s m + m + 1
+  cxd b0 = shfl_c(gmask, l0, dn, P), b1 = shfl_c(gmask, l1, dn, P);  // rows s m - 2, s m - 1
+  if (s == P - 1) {
+    a0 = cmul(a0, ph);
+    a1 = cmul(a1, ph);
+  }
+  if (s == 0) {
+    b0 = cmul(b0, cconj(ph));
+    b1 = cmul(b1, cconj(ph));
+  }
+  cxd w0 = b0, w1 = b1, w2 = f0, w3 = f1, w4 = sb[2];
+#pragma unroll 2
+  for (int i = 0; i < m; ++i) {
+    const double c0 = DS(s, i, n, 0), c1 = DS(s, i, n, 1), c2 = DS(s, i, n, 2), c3 = DS(s, i, n, 3),
+                 c4 = DS(s, i, n, 4);
+    cxd acc = mkc(0, 0);
+    acc = mkc(acc.x + c0 * w0.x, acc.y + c0 * w0.y);
+    acc = mkc(acc.x + c1 * w1.x, acc.y + c1 * w1.y);
+    acc = mkc(acc.x + c2 * w2.x, acc.y + c2 * w2.y);
+    acc = mkc(acc.x + c3 * w3.x, acc.y + c3 * w3.y);
+    acc = mkc(acc.x + c4 * w4.x, acc.y + c4 * w4.y);
+    const int nx = i + 3;
+    const cxd nxt = nx < m ? sb[nx] : (nx == m ? a0 : a1);
+    sb[i] = acc;
+    w0 = w1;
+    w1 = w2;
+    w2 = w3;
+    w3 = w4;
+    w4 = nxt;
+  }
+}
+
+// The solve stage on one column, for MODE COL_SOLVE (and COL_SHIFT: the
+// exact_shift shift alone) with the lines and every intermediate in shared
+// memory: no scratch column of V is written and read back.
+//   EXACT: shift_unweighted (src/hst_equations.f90:263-293) of old1, old2,
+//          rhs1, rhs2, one line at a time: D0 solve with the wrap at t
+//          (factored table), node phase exp(-i gx y), D0 stencil with the
+//          ghost images at t + dt_sub; old1, old2 back to OLD1, OLD2.
+//   then linsolve (:298-326): D2V and ETA solves, v with its ghost rows to
+//   V2, D1 stencil of v and the DY solve (table) in place, u and w, V1 and
+//   V3 with their ghost rows.
+template <int P, bool EXACT, bool SHIFT_ONLY>
+__device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int col, int s, cxd* bufA, cxd* bufB,
+                                                  double* fac) {
+  const Geometry& g = a.g;
+  const int ny = g.ny, nz = g.nz, nzT = g.nzT, m = g.m;
+  LineGeom G;
+  G.n = ny;
+  G.m = m;
+  G.MS = g.MS;
+  G.P = P;
+  G.invm = (unsigned)((1u << 20) + m - 1) / (unsigned)m;
+  const unsigned gmask = group_mask(P);
+  const int ix = col / nzT, iz = col - ix * nzT - nz;
+  const bool c00 = (ix == 0 && iz == 0);
+  const double al = a.ps.alfa0 * ix, be = a.ps.beta0 * iz;
+  const double kk = al * al + be * be;
+  const SubstepScalars& sc = a.sc;
+  const size_t cb = (size_t)col * g.rows + 2;  // row 0 of the column
+  const SlabDer DS = {a.derS, m, P};
+  cxd* const sA = bufA + s * G.MS;  // this lane's slab
+  cxd* const sB = bufB + s * G.MS;
+
+  if (EXACT) {
+    const double th0 = al * sc.sx_t + be * sc.sz_t;
+    const double gx = al * sc.dgx + be * sc.dgz;
+    const cxd phs = cexpi(-(al * sc.sx_n + be * sc.sz_n));
+    // the node phase of the slab's first row; on a uniform grid the next
+    // rows follow by one complex product each (dy = ly / ny apart)
+    const cxd e0 = cexpi(-gx * a.y[s * m + 2]);
+    const cxd estep = sc.yuni ? cexpi(-gx * (sc.ytile / 32.0)) : mkc(1.0, 0.0);
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+      // q = 0, 1: old1, old2 (back to OLD1, OLD2 through bufA); 2: rhs1
+      // (kept in bufA); 3: rhs2 (kept in bufB)
+      cxd* X = q == 3 ? bufB : bufA;
+      cxd* sX = q == 3 ? sB : sA;
+      const double2* src = q == 0 ? a.O1 : (q == 1 ? a.O2 : (q == 2 ? a.R1 : a.R2));
+      for (int r = s; r < ny; r += P) X[G.at(r)] = src[cb + r];
+      __syncwarp(gmask);
+      {
+        cxd* const bufs[1] = {X};
+        group_solve_d0<P, 1>(th0, a.d0tab, G, bufs, s, gmask);
+      }
+      __syncwarp(gmask);
+      cxd e = e0;
+      for (int i = 0; i < m; ++i) {
+        if (!sc.yuni && i > 0) e = cexpi(-gx * a.y[s * m + i + 2]);
+        sX[i] = cmul(sX[i], e);
+        e = cmul(e, estep);
+      }
+      __syncwarp(gmask);
+      slab_stencil<P>(0, DS, sX, m, s, phs, gmask);
+      __syncwarp(gmask);
+      if (q < 2 || SHIFT_ONLY) {
+        double2* dst = q == 0 ? a.O1 : (q == 1 ? a.O2 : (q == 2 ? a.R1 : a.R2));
+        for (int r = s; r < ny; r += P) dst[cb + r] = X[G.at(r)];
+        __syncwarp(gmask);
+      }
+    }
+    if (SHIFT_ONLY) return;
+  } else {
+    for (int r = s; r < ny; r += P) {
+      bufA[G.at(r)] = a.R1[cb + r];
+      bufB[G.at(r)] = a.R2[cb + r];
+    }
+    __syncwarp(gmask);
+  }
+
+  // ---- implicit solves (linsolve, src/hst_equations.f90:298-326)
+  const double thn = al * sc.sx_n + be * sc.sz_n;
+  const cxd phn = cexpi(-thn);
+  group_solve<P>(K_D2V, sc.lambda, a.ps.ni, kk, thn, DS, G, bufB, fac, s, gmask);
+  __syncwarp(gmask);
+  group_solve<P>(K_ETA, sc.lambda, a.ps.ni, kk, thn, DS, G, bufA, fac, s, gmask);
+  __syncwarp(gmask);
+  store_with_ghosts<P>(a.V2 + (size_t)col * g.rows, bufB, G, ny, phn, s, c00);
+  // D1 v through the ghost rows, then D0 (dv/dy) = D1 v (KIND_DY); the (0,0)
+  // column's v is zero
+  if (c00)
+    for (int i = 0; i < m; ++i) sB[i] = mkc(0, 0);
+  __syncwarp(gmask);
+  slab_stencil<P>(1, DS, sB, m, s, phn, gmask);
+  __syncwarp(gmask);
+  {
+    cxd* const bufs[1] = {bufB};
+    group_solve_d0<P, 1>(thn, a.d0tab, G, bufs, s, gmask);
+  }
+  __syncwarp(gmask);
+  // u, w from eta and dv/dy, into bufA (u) and bufB (w)
+  const double rkk = c00 ? 0.0 : 1.0 / kk;
+  for (int i = 0; i < m; ++i) {
+    const cxd eta = sA[i], dv = sB[i];
+    cxd u, w;
+    if (c00) {
+      u = mkc(eta.x, 0.0);
+      w = mkc(eta.y, 0.0);
+    } else {
+      // (i alfa dv - i beta eta) / k2, (i beta dv + i alfa eta) / k2
+      u = mkc((-al * dv.y + be * eta.y) * rkk, (al * dv.x - be * eta.x) * rkk);
+      w = mkc((-be * dv.y - al * eta.y) * rkk, (be * dv.x + al * eta.x) * rkk);
+    }
+    sA[i] = u;
+    sB[i] = w;
+  }
+  __syncwarp(gmask);
+  store_with_ghosts<P>(a.V1 + (size_t)col * g.rows, bufA, G, ny, phn, s, false);
+  store_with_ghosts<P>(a.V3 + (size_t)col * g.rows, bufB, G, ny, phn, s, false);
+}
+
+// One group of P lanes per Fourier column, every intermediate in shared
+// memory, the factor scratch in shared memory after the lines (the fused
+// stage, the streamed right-hand sides, and the solve stage when the context
+// has no global factor scratch).
+template <int P, bool EXACT, bool NONLIN, int MODE>
+__global__ void k_column(ColumnArgs a) {
+  extern __shared__ double smem_d[];
+  const Geometry& g = a.g;
+  const int groups = blockDim.x / P;
+  const int grp = threadIdx.x / P, s = threadIdx.x - grp * P;
+  const int col = blockIdx.x * groups + grp;
+  if (col >= g.ncol) return;
+  const int mi = g.m - 2;
+  const int lineN = P * g.MS;
+  constexpr int NL = (EXACT && MODE == COL_FUSED) ? 3 : 2;  // lines held
+  const size_t per_group = (size_t)NL * lineN * 2 + (size_t)mi * 4 * P;  // doubles
+  double* base = smem_d + per_group * grp;
+  cxd* bufA = reinterpret_cast<cxd*>(base);
+  cxd* bufB = bufA + lineN;
+  cxd* bufC = bufB + lineN;  // EXACT and COL_FUSED only
+  column_body<P, EXACT, NONLIN, MODE>(a, col, s, bufA, bufB, bufC, base + (size_t)NL * lineN * 2);
+}
+
+// The solve stage (SHIFT_ONLY: the exact_shift shift alone) on a persistent
+// grid: each group of P lanes walks the columns col, col + gridDim.x groups,
+// ...; shared memory holds only the group's two lines, and the group's
+// factor scratch is its own slice of a.facg in global memory, rewritten
+// column after column (so it stays in L2).  Fewer bytes of shared memory a
+// warp let more warps share an SM.
+template <int P, bool EXACT, bool SHIFT_ONLY>
+#ifndef COLSOLVE_MINB
+#define COLSOLVE_MINB 8  // 128 registers: up to 16 single-warp blocks an SM
+#endif
+__global__ void __launch_bounds__(64, COLSOLVE_MINB) k_column_solve(ColumnArgs a) {
+  extern __shared__ double smem_d[];
+  const Geometry& g = a.g;
+  const int groups = blockDim.x / P;
+  const int grp = threadIdx.x / P, s = threadIdx.x - grp * P;
+  const int lineN = P * g.MS;
+  const size_t facn = (size_t)(g.m - 2) * 4 * P;
+  const size_t per_group = (size_t)2 * lineN * 2 + (a.facg ? 0 : facn);  // doubles
+  cxd* bufA = reinterpret_cast<cxd*>(smem_d + per_group * grp);
+  cxd* bufB = bufA + lineN;
+  const int slot = blockIdx.x * groups + grp;
+  // the factor scratch: the group's slice of a.facg, or after its lines
+  double* fac = a.facg ? a.facg + (size_t)slot * facn : reinterpret_cast<double*>(bufB + lineN);
+  for (int col = slot; col < g.ncol; col += gridDim.x * groups)
+    column_solve_body<P, EXACT, SHIFT_ONLY>(a, col, s, bufA, bufB, fac);
+}
+
 // --------------------------------------------------------- k_line_solve ----
 // line_solve (src/hst_linsolve.f90:147-233) for every Fourier column.
 template <int P>
@@ -406,6 +616,7 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
   const double2* Vg[3] = {a.V1, a.V2, a.V3};
   // lane 0 queues the copies of tile t into stage t & 1
   const QT* Qg = reinterpret_cast<const QT*>(a.Q);
+  const QT* Qgg = reinterpret_cast<const QT*>(a.Qg);
   constexpr unsigned QE = sizeof(QT);
   auto issue = [&](int t) {
     const int stg = t & 1;
@@ -420,9 +631,12 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
       QT* D = reinterpret_cast<QT*>(S + 3 * RT_W) + p * RT_W;
       const int lo = r0 - 2, hi = r0 + 34;
       const int m0 = lo < 0 ? 0 : lo, m1 = hi > ny ? ny : hi;
-      if (lo < 0) bulk_g2s(D, Qc + ny + lo, (unsigned)(-lo) * QE, &bar[stg]);
+      // the rows beyond the box: the wrapped interior rows (their phase is
+      // applied in tq), or the ghost rows' own spectra
+      const QT* Qgc = Qgg ? Qgg + ((size_t)p * g.ncol + col) * 4 : nullptr;
+      if (lo < 0) bulk_g2s(D, Qgc ? Qgc : Qc + ny + lo, (unsigned)(-lo) * QE, &bar[stg]);
       bulk_g2s(D + (m0 - lo), Qc + m0, (unsigned)(m1 - m0) * QE, &bar[stg]);
-      if (hi > ny) bulk_g2s(D + (ny - lo), Qc, (unsigned)(hi - ny) * QE, &bar[stg]);
+      if (hi > ny) bulk_g2s(D + (ny - lo), Qgc ? Qgc + 2 : Qc, (unsigned)(hi - ny) * QE, &bar[stg]);
     }
     bulk_g2s(S + 9 * RT_W, a.O1 + cbase + 2 + r0, 32 * 16, &bar[stg]);
     bulk_g2s(S + 9 * RT_W + 32, a.O2 + cbase + 2 + r0, 32 * 16, &bar[stg]);
@@ -464,6 +678,7 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
     auto tq = [&](int p, int j) -> QT {
       const QT q = SQ[p * RT_W + lane + j];
       const int row = r + j - 2;
+      if (Qgg) return q;
       if (row < 0) return cmul(q, cconj(ph_q));
       if (row >= ny) return cmul(q, ph_q);
       return q;
@@ -491,6 +706,10 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
 }
 
 // -------------------------------------------------------------- launchers ----
+size_t column_lines_bytes(const Geometry& g) { return (size_t)2 * g.P * g.MS * sizeof(double2); }
+
+size_t column_fac_doubles(const Geometry& g) { return (size_t)(g.m - 2) * 4 * g.P; }
+
 size_t column_smem_bytes(const Geometry& g, int exact) {
   size_t lineN = (size_t)g.P * g.MS;
   return ((exact ? 3 : 2) * lineN * 2 + (size_t)(g.m - 2) * 4 * g.P) * sizeof(double);
@@ -520,16 +739,37 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
     return cudaGetLastError();
   }
   // 32 or 64 threads, fewer groups when their shared memory would not fit
-  const size_t per = column_smem_bytes(g, EXACT && MODE == COL_FUSED);
+  // the solve stage runs persistent; its factor scratch is in global memory
+  // when the context has one (HST_COLUMN_GFAC), else in shared memory
+  // the persistent solve stage when the context keeps the factor scratch in
+  // global memory, else the one-column-per-group kernel
+  const bool gfac = (MODE == COL_SOLVE || (MODE == COL_SHIFT && EXACT)) && a.facg != nullptr;
+  const size_t per = gfac ? column_lines_bytes(g) + (a.facg ? 0 : column_fac_doubles(g) * sizeof(double))
+                          : column_smem_bytes(g, EXACT && MODE == COL_FUSED);
   int groups = (P >= 32 ? 32 : 64) / P;
   if (groups < 1) groups = 1;
   while (groups > 1 && per * groups > 200 * 1024) groups >>= 1;
   if (per * groups > 200 * 1024) return cudaErrorInvalidValue;
   const int T = groups * P;
   size_t smem = per * groups;
-  smem_limit(*a.dstate, k_column<P, EXACT, NONLIN, MODE>, 200 * 1024);
   int blocks = (g.ncol + groups - 1) / groups;
-  k_column<P, EXACT, NONLIN, MODE><<<blocks, T, smem, st>>>(a);
+  if (gfac) {
+    auto kern = k_column_solve<P, EXACT, MODE == COL_SHIFT>;
+    smem_limit(*a.dstate, kern, 200 * 1024);
+    // persistent: the blocks that are resident at once (at most 16 warps an
+    // SM), and no more groups than the scratch has slices for
+    int per_sm = blocks_per_sm(*a.dstate, kern, T, smem);
+    per_sm = std::min(per_sm, std::max(1, 16 * 32 / T));
+    const int nsm = a.dstate->nsm > 0 ? a.dstate->nsm : 148;
+    blocks = std::min(blocks, per_sm * nsm);
+    if (a.facg) blocks = std::min(blocks, a.fac_groups / groups);
+    if (blocks < 1) return cudaErrorInvalidValue;
+    kern<<<blocks, T, smem, st>>>(a);
+    return cudaGetLastError();
+  }
+  auto kern = k_column<P, EXACT, NONLIN, MODE>;
+  smem_limit(*a.dstate, kern, 200 * 1024);
+  kern<<<blocks, T, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -565,6 +805,7 @@ cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysSca
   a.R1 = d.F[5];
   a.R2 = d.F[6];
   a.Q = d.Q;
+  a.Qg = d.Qg;
   a.der = d.der;
   a.derS = d.derS;
   a.d0tab = d.d0tab;
@@ -572,6 +813,9 @@ cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysSca
   a.gdamp = d.gdamp;
   a.err = d.err;
   a.dstate = &d;
+  a.facg = d.facg;
+  a.fac_groups = d.facg ? (int)std::min<size_t>(d.facg_doubles / column_fac_doubles(g), 1u << 30) : 0;
+  if (a.fac_groups < 1) a.facg = nullptr;
   {
     const char* e = std::getenv("HST_RHS_TILED");
     a.tiled = !(e && std::atoi(e) == 0);

@@ -182,6 +182,7 @@ __global__ void k_stats_final(int nblk, const double* __restrict__ pm, const dou
 template <typename QT>
 __global__ void __launch_bounds__(32 * ST_WARPS) k_pressure_rhs(Geometry g, PhysScalars ps, double s2now, double sx,
                                                                 double sz, const QT* __restrict__ Q,
+                                                                const QT* __restrict__ Qg,
                                                                 const double2* __restrict__ V2,
                                                                 const double* __restrict__ der,
                                                                 double2* __restrict__ R) {
@@ -204,10 +205,16 @@ __global__ void __launch_bounds__(32 * ST_WARPS) k_pressure_rhs(Geometry g, Phys
 #pragma unroll
       for (int j = 0; j < 5; ++j) {
         const int q = r + j - 2;
-        const QT qr = Qc[(size_t)p * qs + (q < 0 ? q + ny : (q >= ny ? q - ny : q))];
-        cxd v = mkc((double)qr.x, (double)qr.y);
-        if (q < 0) v = cmul(v, cconj(ph));
-        if (q >= ny) v = cmul(v, ph);
+        cxd v;
+        if (Qg && (q < 0 || q >= ny)) {  // the ghost rows' own spectra
+          const QT qr = Qg[((size_t)p * g.ncol + col) * 4 + (q < 0 ? q + 2 : q - ny + 2)];
+          v = mkc((double)qr.x, (double)qr.y);
+        } else {
+          const QT qr = Qc[(size_t)p * qs + (q < 0 ? q + ny : (q >= ny ? q - ny : q))];
+          v = mkc((double)qr.x, (double)qr.y);
+          if (q < 0) v = cmul(v, cconj(ph));
+          if (q >= ny) v = cmul(v, ph);
+        }
         const double e0 = derv(der, ny, r, 0, j - 2), e1 = derv(der, ny, r, 1, j - 2), e2 = derv(der, ny, r, 2, j - 2);
         d0 = mkc(d0.x + e0 * v.x, d0.y + e0 * v.y);
         d1 = mkc(d1.x + e1 * v.x, d1.y + e1 * v.y);
@@ -256,9 +263,10 @@ cudaError_t launch_pressure_rhs(const Geometry& g, const DeviceState& d, const P
   const int blocks = (g.ncol + ST_WARPS - 1) / ST_WARPS;
   if (g.mp)
     k_pressure_rhs<float2><<<blocks, 32 * ST_WARPS, 0, st>>>(g, ps, s2now, sx, sz, reinterpret_cast<const float2*>(d.Q),
-                                                             d.F[1], d.der, d.F[5]);
+                                                             reinterpret_cast<const float2*>(d.Qg), d.F[1], d.der,
+                                                             d.F[5]);
   else
-    k_pressure_rhs<double2><<<blocks, 32 * ST_WARPS, 0, st>>>(g, ps, s2now, sx, sz, d.Q, d.F[1], d.der, d.F[5]);
+    k_pressure_rhs<double2><<<blocks, 32 * ST_WARPS, 0, st>>>(g, ps, s2now, sx, sz, d.Q, d.Qg, d.F[1], d.der, d.F[5]);
   return cudaGetLastError();
 }
 

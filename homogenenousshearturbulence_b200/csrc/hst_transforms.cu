@@ -52,12 +52,13 @@ template <typename C>
 struct ZinvSrc {
   const double2* __restrict__ col;  // V + (ix nzT) rows + 2 + y0: row y0 of iz = -nz
   int rows, nz, NZ;
+  int gap;  // the edge view: rows -2, -1 at 0, 1 and ny, ny+1 at gap + 2, gap + 3
   __device__ __forceinline__ C operator()(int yi, int kz) const {
     int iz;
     if (kz <= nz) iz = kz;
     else if (kz >= NZ - nz) iz = kz - NZ;
     else return C{0, 0};
-    return to_c<C>(col[(size_t)(iz + nz) * rows + yi]);
+    return to_c<C>(col[(size_t)(iz + nz) * rows + yi + (yi >= 2 ? gap : 0)]);
   }
 };
 template <typename C>
@@ -82,7 +83,8 @@ __device__ __forceinline__ void zinv_body(const Geometry& g, const double2* __re
   const int yt = blockIdx.x, ix = blockIdx.y, c = blockIdx.z;
   const int Ty = g.Ty, NZ = g.nzd, nyT = g.ny / Ty;
   const double2* V = c == 0 ? V0 : (c == 1 ? V1 : V2);
-  const ZinvSrc<C> src = {V + (size_t)ix * g.nzT * g.rows + 2 + yt * Ty, g.rows, g.nz, NZ};
+  const ZinvSrc<C> src = {V + (size_t)ix * g.nzT * g.rows + (g.edge_gap ? 0 : 2) + yt * Ty, g.rows, g.nz, NZ,
+                          g.edge_gap};
   const TileDst<C> dst = {Z + (((size_t)c * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
   fft_sel<NT, +1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
 }
@@ -212,12 +214,17 @@ struct ProdSrc {
 // launch bounds of k_xprod: 6 NX / PPT threads; the 8-point plan at 384
 // is held to 72 registers so that three 288-thread blocks fit an SM, the
 // FP32 32-point plan at 1536 to two blocks
-constexpr int xprod_threads(int NT, int PPT) { return PPT <= 8 ? (NT == 384 ? 288 : 640) : (NT == 1536 ? 288 : 320); }
+constexpr int xprod_threads(int NT, int PPT) {
+  return PPT <= 8 ? (NT == 384 ? 288 : (NT == 768 ? 576 : 640)) : (NT == 1536 ? 288 : 320);
+}
+#ifndef XPROD_MINB_768
+#define XPROD_MINB_768 2
+#endif
 #ifndef XPROD_MINB_F32
 #define XPROD_MINB_F32 4
 #endif
 constexpr int xprod_min_blocks(int NT, int PPT, int es) {
-  return PPT <= 8 && NT == 384 ? (es == 8 ? XPROD_MINB_F32 : XPROD_MINB) : (NT == 1536 && es == 8 ? 2 : 1);
+  return PPT <= 8 && NT == 384 ? (es == 8 ? XPROD_MINB_F32 : XPROD_MINB) : ((NT == 1536 || NT == 768) && es == 8 ? 2 : (NT == 768 && PPT <= 8 ? XPROD_MINB_768 : 1));
 }
 
 constexpr int XPROD_WAIT_LIMIT = 1 << 22;  // polls of the tile's TMA barrier before giving up
@@ -231,6 +238,12 @@ __host__ __device__ inline int xprod_stage_off(int NX) { return 6 * ls_padded(NX
 __host__ __device__ inline size_t xprod_tma_smem(int NX, int nxB, size_t elem) {
   return ((size_t)xprod_stage_off(NX) + 12 * (size_t)nxB + 2) * elem + 128;
 }
+// At 768 points the staging tiles live inside the six lines instead (the
+// tile in where lines 3..5 are, which the three inverse lines never touch;
+// the tile out over the lines once they have been read), so that a block
+// needs 6 padded lines of shared memory and two blocks share an SM
+__host__ __device__ constexpr bool xprod_alias(int NT, int PPT) { return PPT <= 8 && NT == 768; }
+__host__ __device__ inline size_t xprod_alias_smem(int NX, size_t elem) { return (size_t)6 * ls_padded(NX) * elem + 128; }
 
 template <int NT, int PPT, typename C>
 __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, PPT, (int)sizeof(C)))
@@ -251,12 +264,17 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   const size_t cs = (size_t)NZ * nyT * nxB * Ty;
   const size_t tile = ((size_t)yt * NZ + kz) * nxB * Ty;
   const LT L = {sh, LS};
-  C* stg = sh + xprod_stage_off(NX);
-  if constexpr (JF) stg += ((128u - (smem_u32(stg) & 127u)) & 127u) / sizeof(C);
+  constexpr bool ALIAS = xprod_alias(NT, PPT);
+  auto align128 = [](C* q) { return q + ((128u - (smem_u32(q) & 127u)) & 127u) / sizeof(C); };
+  C* stg = ALIAS ? sh + 3 * LS : sh + xprod_stage_off(NX);
+  if constexpr (JF) stg = align128(stg);
+  C* const stg_out = ALIAS ? align128(sh) : stg;
+  __shared__ uint64_t bar_al;
+  __shared__ int tile_ok_al;
   // u + i v of both rows and w0 + i w1 on the physical x grid
   if constexpr (JF) {
-    uint64_t* bar = reinterpret_cast<uint64_t*>(stg + 12 * nxB);
-    int& tile_ok = *reinterpret_cast<int*>(stg + 12 * nxB + 1);
+    uint64_t* bar = ALIAS ? &bar_al : reinterpret_cast<uint64_t*>(stg + 12 * nxB);
+    int& tile_ok = ALIAS ? tile_ok_al : *reinterpret_cast<int*>(stg + 12 * nxB + 1);
     if ((smem_u32(stg) & 127u) != 0) {  // never taken: the staging tile is aligned above
       if (threadIdx.x == 0) atomicExch(err, 1);
       return;
@@ -304,6 +322,38 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   fft_sel<NT, -1, PPT, true, true, JF>(NX, 6, JF ? twx + NX : twx, sh, ps6, L);
   __syncthreads();
   // separate the two real transforms of each line, keep kx = 0..nx
+  if constexpr (ALIAS) {
+    // the tile out overlays the lines: every thread reads its (at most two,
+    // as 3 nxB <= NX <= 2 blockDim) entries first, then writes
+    C zk[2][2], zm[2][2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int e = threadIdx.x + k * blockDim.x;
+      if (e < nxB * 3) {
+        const int pl = e / nxB, ix = e - pl * nxB;
+#pragma unroll
+        for (int yy = 0; yy < 2; ++yy) {
+          zk[k][yy] = L(pl + 3 * yy, ix);
+          zm[k][yy] = L(pl + 3 * yy, ix == 0 ? 0 : NX - ix);
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int e = threadIdx.x + k * blockDim.x;
+      if (e < nxB * 3) {
+        const int pl = e / nxB, ix = e - pl * nxB;
+#pragma unroll
+        for (int yy = 0; yy < 2; ++yy) {
+          const C Zk = zk[k][yy], Zm = zm[k][yy];
+          const T h = T(0.5);
+          stg_out[((2 * pl) * nxB + ix) * 2 + yy] = C{h * (Zk.x + Zm.x), h * (Zk.y - Zm.y)};
+          stg_out[((2 * pl + 1) * nxB + ix) * 2 + yy] = C{h * (Zk.y + Zm.y), h * (Zm.x - Zk.x)};
+        }
+      }
+    }
+  } else
   for (int e = threadIdx.x; e < nxB * 3; e += blockDim.x) {
     int pl = e / nxB, ix = e - pl * nxB;
 #pragma unroll
@@ -328,7 +378,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
     fence_proxy_async();
     __syncthreads();
     if (threadIdx.x == 0) {
-      tma_store_4d(&tmP, 2 * yi0, 0, yt * NZ + kz, 0, stg);
+      tma_store_4d(&tmP, 2 * yi0, 0, yt * NZ + kz, 0, stg_out);
       bulk_commit();
       bulk_wait_read_all();
     }
@@ -491,9 +541,34 @@ cudaError_t make_transform_maps(const Geometry& g, DeviceState& d) {
                      which == 0 ? (void*)d.Z : (void*)d.Pp, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    if (d.Zg) {  // the ghost rows' buffers: one tile of four rows
+      cuuint64_t dg[4] = {8, (cuuint64_t)g.nxB, (cuuint64_t)g.nzd, comps};
+      cuuint64_t sg[3] = {es * 4, es * 4 * g.nxB, es * 4 * g.nxB * g.nzd};
+      r = enc(which == 0 ? &d.tmZg : &d.tmPpg, g.mp ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+              which == 0 ? (void*)d.Zg : (void*)d.Ppg, dg, sg, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    }
   }
   d.maps = true;
   return cudaSuccess;
+}
+
+bool edge_rows_needed(const Geometry& g, bool s2_active) { return s2_active && g.nzd <= 3 * g.nz; }
+
+// The view of the four ghost rows: the same transforms with ny = Ty = 4 on
+// the edge buffers
+static void edge_view(const Geometry& g, const DeviceState& d, Geometry& ge, DeviceState& de) {
+  ge = g;
+  ge.ny = 4;
+  ge.Ty = 4;
+  ge.edge_gap = g.ny;
+  de = d;
+  de.Z = d.Zg;
+  de.Pp = d.Ppg;
+  de.Q = d.Qg;
+  de.tmZ = d.tmZg;
+  de.tmPp = d.tmPpg;
 }
 
 // -------------------------------------------------------------- launchers ----
@@ -551,7 +626,7 @@ static void big_smem(const DeviceState& d, K k) {
 
 bool mp_length_ok(int n) { return n == 96 || n == 192 || n == 384 || n == 768 || n == 1536; }
 
-cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st) {
+static cudaError_t launch_zinv_main(const Geometry& g, const DeviceState& d, cudaStream_t st) {
   const int pts = g.nzd * g.Ty;
   const dim3 grid(g.ny / g.Ty, g.nxB, 3);
   if (g.mp) {
@@ -584,7 +659,7 @@ cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st
   return cudaGetLastError();
 }
 
-cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st) {
+static cudaError_t launch_zfwd_main(const Geometry& g, const DeviceState& d, cudaStream_t st) {
   const int pts = g.nzd * g.Ty;
   const dim3 grid(g.ny / g.Ty, g.nxB, 6);
   if (g.mp) {
@@ -613,16 +688,16 @@ cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st
   return cudaGetLastError();
 }
 
-cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int want_cfl,
-                         cudaStream_t st) {
+static cudaError_t launch_xprod_main(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int want_cfl,
+                                     cudaStream_t st) {
   const int NX = 2 * g.nxd;
   const int pts = 6 * NX;
   if (xprod_uses_maps(g) != d.maps) return cudaErrorInvalidValue;
   const dim3 grid(g.ny / 2, g.nzd);
   if (g.mp) {
     typedef float2 C;
-    const size_t smem =
-        xprod_uses_maps(g) ? xprod_tma_smem(NX, g.nxB, sizeof(C)) : (size_t)6 * (NX + 1) * sizeof(C);
+    const size_t smem = !xprod_uses_maps(g) ? (size_t)6 * (NX + 1) * sizeof(C)
+                        : (NX == 768 ? xprod_alias_smem(NX, sizeof(C)) : xprod_tma_smem(NX, g.nxB, sizeof(C)));
     const C* Z = reinterpret_cast<const C*>(d.Z);
     C* Pp = reinterpret_cast<C*>(d.Pp);
 #define HST_XPROD(NT, PPT)                                                                                    \
@@ -636,7 +711,9 @@ cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScal
     return cudaGetLastError();
   }
   typedef double2 C;
-  const size_t smem = xprod_uses_maps(g) ? xprod_tma_smem(NX, g.nxB, sizeof(C)) : (size_t)6 * (NX + 1) * sizeof(C);
+  const size_t smem = !xprod_uses_maps(g) ? (size_t)6 * (NX + 1) * sizeof(C)
+                      : (NX == 768 && g.pptx == 8 ? xprod_alias_smem(NX, sizeof(C))
+                                                  : xprod_tma_smem(NX, g.nxB, sizeof(C)));
 #define HST_XPROD(NT, PPT)                                                                                    \
   {                                                                                                           \
     big_smem(d, k_xprod<NT, PPT, C>);                                                                            \
@@ -646,6 +723,34 @@ cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScal
   HST_FFT_DISPATCH(NX, pts, g.pptx == 8, HST_XPROD);
 #undef HST_XPROD
   return cudaGetLastError();
+}
+
+// each transform of the interior rows, then (when the context keeps them)
+// of the four ghost rows; the ghost rows take no part in the CFL number
+cudaError_t launch_zinv(const Geometry& g, const DeviceState& d, cudaStream_t st) {
+  cudaError_t e = launch_zinv_main(g, d, st);
+  if (e != cudaSuccess || !d.Qg) return e;
+  Geometry ge;
+  DeviceState de;
+  edge_view(g, d, ge, de);
+  return launch_zinv_main(ge, de, st);
+}
+cudaError_t launch_xprod(const Geometry& g, const DeviceState& d, const PhysScalars& ph, int want_cfl,
+                         cudaStream_t st) {
+  cudaError_t e = launch_xprod_main(g, d, ph, want_cfl, st);
+  if (e != cudaSuccess || !d.Qg) return e;
+  Geometry ge;
+  DeviceState de;
+  edge_view(g, d, ge, de);
+  return launch_xprod_main(ge, de, ph, 0, st);
+}
+cudaError_t launch_zfwd(const Geometry& g, const DeviceState& d, cudaStream_t st) {
+  cudaError_t e = launch_zfwd_main(g, d, st);
+  if (e != cudaSuccess || !d.Qg) return e;
+  Geometry ge;
+  DeviceState de;
+  edge_view(g, d, ge, de);
+  return launch_zfwd_main(ge, de, st);
 }
 
 }  // namespace hst

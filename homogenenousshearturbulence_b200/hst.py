@@ -16,12 +16,15 @@ from __future__ import annotations
 
 import ctypes as ct
 import math
+import os
 import pathlib
 
 import numpy as np
 
 PKG = pathlib.Path(__file__).resolve().parent
-LIB_PATH = PKG / "libhst_gpu.so"
+# HST_GPU_LIB: another build of the library (e.g. one compiled with other
+# launch bounds, to compare); the in-tree build by default
+LIB_PATH = pathlib.Path(os.environ.get("HST_GPU_LIB", str(PKG / "libhst_gpu.so")))
 
 V1, V2, V3, OLD1, OLD2, RHS1, RHS2 = range(7)
 KIND_D2V, KIND_ETA, KIND_POISSON, KIND_D0, KIND_DY = 1, 2, 3, 4, 5
@@ -382,7 +385,7 @@ class Solver:
     def s2_integral(self, t1, t2):
         return lib().hst_gpu_s2_integral(self._h, float(t1), float(t2))
 
-    KERNEL_CLASSES = ("zinv", "xprod", "zfwd", "column", "line_solve", "ghosts", "rhs")
+    KERNEL_CLASSES = ("zinv", "xprod", "zfwd", "column", "line_solve", "ghosts", "rhs", "shift")
 
     def set_profiling(self, on: bool):
         self._check(lib().hst_gpu_set_profiling(self._h, int(bool(on))), "set_profiling")

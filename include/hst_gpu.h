@@ -315,7 +315,8 @@ double hst_gpu_s2_integral(const hst_ctx* ctx, double t1, double t2);
 #define HST_KC_LINE_SOLVE 4 /* hst_gpu_line_solve */
 #define HST_KC_GHOSTS 5     /* hst_gpu_fill_ghosts */
 #define HST_KC_RHS 6        /* the right-hand sides streamed row by row (when the column stage is split) */
-#define HST_KC_N 7
+#define HST_KC_SHIFT 7      /* the exact_shift shear shift, when it runs as a kernel of its own */
+#define HST_KC_N 8
 
 /* Per-kernel device time: with profiling on, every launch is bracketed by
  * two CUDA events on the context's stream; hst_gpu_kernel_times waits for

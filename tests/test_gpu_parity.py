@@ -515,7 +515,10 @@ def test_outstats_sums_match_oracle(deck_over):
         assert abs(g1[name] - r[k]) <= 1e-10 * scale, (name, g1[name], r[k])
     assert g1["ncol_damped"] == r[15]
     if deck_over:
-        assert r[15] > 0 and r[13] > 0
+        assert r[15] > 0
+        # the hard mask leaves no energy in the damped columns; the soft
+        # damping only slows it down
+        assert (r[13] == 0.0) if deck_over.get("damp_hard") else (r[13] > 0 and r[14] > 0)
     assert np.abs(e1 - er).max() <= 1e-10 * np.abs(er).max()
     # the box averages of outstats follow from the sums
     st = s.outstats()

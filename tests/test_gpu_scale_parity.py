@@ -125,6 +125,26 @@ def test_768_plans_parity(prec, tol, axis):
     assert err <= tol, err
 
 
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+@pytest.mark.parametrize("exact", [False, True])
+def test_s2_edge_modes_parity(prec, tol, exact):
+    """With a spanwise shear S2 and the reference's padding nzd = 3 nz (here
+    nz = 32, nzd = 96) the retained modes iz = +-nz of the products alias the
+    product modes -+2nz, so the products of the ghost rows are not the wrap
+    images of the interior rows' (their phases differ): the ghost rows are
+    transformed themselves, as the reference transforms every row.  30
+    substeps with energy at the edge modes (k0 = 16) against the oracle."""
+    deck = c1_deck(ny=64, re=5000.0, deltat=0.001, exact_shift=exact, s2_amplitude=0.5, s2_period=10.0, nx=31, nz=32)
+    y = oracle.Sim(oracle.params_from_deck(dict(deck, nx=1, nz=1))).y()
+    V0 = hst.random_field(deck["nx"], deck["ny"], deck["nz"], 1.0, 1.0, deck["ly"], y, seed=5, k0=16.0, energy=0.1)
+    s, o = make_pair(dict(deck, precision=prec), V0)
+    assert s.nzd == 3 * s.nz
+    Vg, Vo = run_pair(s, o, deck["deltat"], 10)
+    s.close()
+    err = rel_l2(Vg, Vo)
+    assert err <= tol, err
+
+
 def test_nan_field_is_reported():
     """A field that has gone NaN must not read back a finite CFL number:
     hst_gpu_timestep returns HST_EFINITE (the reference's time loop would go
