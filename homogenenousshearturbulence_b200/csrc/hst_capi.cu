@@ -144,6 +144,12 @@ struct hst_ctx {
   double* h_gdamp;                // pinned staging of gdamp uploads
   unsigned long long* h_cfl;      // pinned CFL read-back
   std::string err;
+  // an ensemble of nmem members in one context (hst_gpu_create_batch): gb, db
+  // the geometry and buffers of all members, which the substep runs on; g, d
+  // the view of the selected member, which every other entry point uses
+  int nmem = 1, member = 0;
+  Geometry gb;
+  DeviceState db;
   std::unordered_set<const void*> configured;  // kernels whose shared-memory limit is raised
   std::unordered_map<uint64_t, int> occupancy;  // resident blocks an SM, per launch shape
   long long launches;
@@ -151,8 +157,10 @@ struct hst_ctx {
   // the column stage as two kernels (right-hand sides streamed row by row,
   // then the solves) or one; HST_COLUMN_FUSED=1 selects the single kernel
   bool column_split;
-  // with exact_shift, the shift as a third kernel before the solves
-  // (HST_SHIFT_SPLIT=1)
+  // with exact_shift, the shift as a third kernel before the solves: on with
+  // the persistent solve stage (slabs of 16 rows or more; 768^2 x 512: shift
+  // 4.4 + solves 4.9 ms against 10.3 ms in one kernel), HST_SHIFT_SPLIT=0 / 1
+  // forces it
   bool shift_split;
   // per-kernel-class CUDA-event accounting (hst_gpu_set_profiling)
   bool prof_on;
@@ -279,6 +287,10 @@ static bool damping_update(hst_ctx* c, double t) {
 }
 
 // ------------------------------------------------------ geometry ----
+#ifndef ZT768
+#define ZT768 0
+#endif
+#define ZT_MAX_THREADS (ZT768 ? 768 : 384)
 static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& why) {
   g.nx = p.nx;
   g.ny = p.ny;
@@ -306,6 +318,7 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
     return HST_EARG;
   }
   g.edge_gap = 0;
+  g.nmem = 1;
   g.nxB = p.nx + 1;
   g.nzT = 2 * p.nz + 1;
   g.rows = p.ny + 4;
@@ -371,7 +384,7 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
   // transform y tile (at most 512 threads for the 8-point z plans)
   g.Ty = 2;
   for (int t : {8, 4}) {
-    if (p.ny % t == 0 && (size_t)t * (g.nzd + 1) * 16 <= 100 * 1024 && (g.pptz != 8 || t * g.nzd / 8 <= 384)) {
+    if (p.ny % t == 0 && (size_t)t * (g.nzd + 1) * 16 <= 100 * 1024 && (g.pptz != 8 || t * g.nzd / 8 <= ZT_MAX_THREADS)) {
       g.Ty = t;
       break;
     }
@@ -418,6 +431,17 @@ static std::vector<double2> twiddles(int n) {
 }
 
 static void free_device(hst_ctx* c) {
+  if (c->nmem > 1) {
+    // the per-member buffers belong to the base; the view only points into them
+    DeviceState& d = c->d;
+    for (int i = 0; i < 7; ++i) d.F[i] = c->db.F[i];
+    d.Z = c->db.Z;
+    d.Pp = c->db.Pp;
+    d.Q = c->db.Q;
+    d.Zg = c->db.Zg;
+    d.Ppg = c->db.Ppg;
+    d.Qg = c->db.Qg;
+  }
   DeviceState& d = c->d;
   for (int i = 0; i < 7; ++i)
     if (d.F[i]) cudaFree(d.F[i]);
@@ -473,18 +497,18 @@ static cudaError_t ensure_facg(hst_ctx* ctx) {
   return cudaSuccess;
 }
 
-extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
-  if (!pin || !out) return HST_EARG;
+static int create_context(const hst_gpu_params* pin, int nmem, hst_ctx** out) {
+  if (!pin || !out || nmem < 1 || nmem > 4096) return HST_EARG;
   *out = nullptr;
   hst_ctx* ctx = new (std::nothrow) hst_ctx();
   if (!ctx) return HST_ENOMEM;
   ctx->p = *pin;
+  ctx->nmem = nmem;
   ctx->launches = 0;
   {
     const char* e = std::getenv("HST_COLUMN_FUSED");
     ctx->column_split = !(e && std::atoi(e) == 1);
-    const char* f = std::getenv("HST_SHIFT_SPLIT");
-    ctx->shift_split = f && std::atoi(f) == 1;
+    ctx->shift_split = false;  // decided once the geometry is known
   }
   ctx->prof_on = false;
   for (int k = 0; k < HST_KC_N; ++k) {
@@ -557,15 +581,16 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   };
   DeviceState& d = ctx->d;
   bool ok = true;
-  for (int i = 0; i < 7 && ok; ++i) ok = alloc((void**)&d.F[i], sizeof(double2) * g.nf);
+  const size_t nm = (size_t)nmem;  // the per-field buffers hold every member
+  for (int i = 0; i < 7 && ok; ++i) ok = alloc((void**)&d.F[i], sizeof(double2) * g.nf * nm);
   const size_t es = g.mp ? sizeof(float2) : sizeof(double2);  // the transforms' complex element
-  ok = ok && alloc((void**)&d.Z, es * 3 * (size_t)g.nzd * g.ny * g.nxB);
-  ok = ok && alloc((void**)&d.Pp, es * 6 * (size_t)g.nzd * g.ny * g.nxB);
-  ok = ok && alloc((void**)&d.Q, es * 6 * (size_t)g.ncol * g.ny);
+  ok = ok && alloc((void**)&d.Z, es * 3 * (size_t)g.nzd * g.ny * g.nxB * nm);
+  ok = ok && alloc((void**)&d.Pp, es * 6 * (size_t)g.nzd * g.ny * g.nxB * nm);
+  ok = ok && alloc((void**)&d.Q, es * 6 * (size_t)g.ncol * g.ny * nm);
   if (hst::edge_rows_needed(g, p.s2_amplitude != 0.0 || p.s2_mean != 0.0)) {
-    ok = ok && alloc((void**)&d.Zg, es * 3 * (size_t)g.nzd * g.nxB * 4);
-    ok = ok && alloc((void**)&d.Ppg, es * 6 * (size_t)g.nzd * g.nxB * 4);
-    ok = ok && alloc((void**)&d.Qg, es * 6 * (size_t)g.ncol * 4);
+    ok = ok && alloc((void**)&d.Zg, es * 3 * (size_t)g.nzd * g.nxB * 4 * nm);
+    ok = ok && alloc((void**)&d.Ppg, es * 6 * (size_t)g.nzd * g.nxB * 4 * nm);
+    ok = ok && alloc((void**)&d.Qg, es * 6 * (size_t)g.ncol * 4 * nm);
   }
   ok = ok && alloc((void**)&d.der, sizeof(double) * 20 * (size_t)ny);
   ok = ok && alloc((void**)&d.derS, sizeof(double) * 20 * (size_t)ny);
@@ -595,7 +620,7 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
     delete ctx;
     return HST_ECUDA;
   }
-  for (int i = 0; i < 7; ++i) cudaMemsetAsync(d.F[i], 0, sizeof(double2) * g.nf, ctx->stream);
+  for (int i = 0; i < 7; ++i) cudaMemsetAsync(d.F[i], 0, sizeof(double2) * g.nf * nm, ctx->stream);
   cudaMemsetAsync(d.cfl, 0, 2 * sizeof(unsigned long long), ctx->stream);
   auto tx = twiddles(2 * g.nxd), tz = twiddles(g.nzd);
   cudaMemcpy(d.der, ctx->der.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice);
@@ -629,8 +654,20 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
   cudaMemcpy(d.twz, tz.data(), sizeof(double2) * tz.size(), cudaMemcpyHostToDevice);
   cudaError_t e = etab;
   if (e == cudaSuccess) e = hst::set_fft_constants();
+  // the base of all members (maps over nmem members), then member 0's view
+  ctx->gb = g;
+  ctx->gb.nmem = nmem;
+  if (e == cudaSuccess) {
+    ctx->db = d;
+    e = hst::make_transform_maps(ctx->gb, ctx->db);
+  }
   if (e == cudaSuccess) e = hst::make_transform_maps(g, d);
   if (e == cudaSuccess) e = ensure_facg(ctx);
+  if (e == cudaSuccess) ctx->db.facg = d.facg, ctx->db.facg_doubles = d.facg_doubles;
+  {
+    const char* f = std::getenv("HST_SHIFT_SPLIT");
+    ctx->shift_split = f ? std::atoi(f) == 1 : ctx->d.facg != nullptr;
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -640,6 +677,43 @@ extern "C" int hst_gpu_create(const hst_gpu_params* pin, hst_ctx** out) {
     return HST_ECUDA;
   }
   *out = ctx;
+  return HST_OK;
+}
+
+extern "C" int hst_gpu_create(const hst_gpu_params* p, hst_ctx** out) { return create_context(p, 1, out); }
+
+extern "C" int hst_gpu_create_batch(const hst_gpu_params* p, int nmem, hst_ctx** out) {
+  return create_context(p, nmem, out);
+}
+
+extern "C" int hst_gpu_members(const hst_ctx* ctx) { return ctx ? ctx->nmem : 0; }
+
+// The view of member m: every per-field pointer offset to its slice of the
+// base buffers, its own TMA maps
+extern "C" int hst_gpu_select_member(hst_ctx* ctx, int m) {
+  if (!ctx || m < 0 || m >= ctx->nmem) return fail(ctx, HST_EARG, "select_member: member %d of %d", m, ctx ? ctx->nmem : 0);
+  if (m == ctx->member) return HST_OK;
+  CK(cudaSetDevice(ctx->device));
+  const Geometry& g = ctx->g;
+  const DeviceState& b = ctx->db;
+  DeviceState& d = ctx->d;
+  const size_t mm = (size_t)m;
+  for (int i = 0; i < 7; ++i) d.F[i] = b.F[i] + mm * g.nf;
+  const size_t es = g.mp ? 1 : 2;  // complex elements of the transforms per double2 slot: FP32 ones pack two
+  auto off = [&](double2* base, size_t elems) -> double2* {
+    if (!base) return nullptr;
+    return g.mp ? reinterpret_cast<double2*>(reinterpret_cast<float2*>(base) + mm * elems) : base + mm * elems;
+  };
+  (void)es;
+  d.Z = off(b.Z, 3 * (size_t)g.nzd * g.ny * g.nxB);
+  d.Pp = off(b.Pp, 6 * (size_t)g.nzd * g.ny * g.nxB);
+  d.Q = off(b.Q, 6 * (size_t)g.ncol * g.ny);
+  d.Zg = off(b.Zg, 3 * (size_t)g.nzd * g.nxB * 4);
+  d.Ppg = off(b.Ppg, 6 * (size_t)g.nzd * g.nxB * 4);
+  d.Qg = off(b.Qg, 6 * (size_t)g.ncol * 4);
+  CK(cudaStreamSynchronize(ctx->stream));  // the maps are kernel arguments of work already queued
+  CK(hst::make_transform_maps(g, d));
+  ctx->member = m;
   return HST_OK;
 }
 
@@ -962,6 +1036,7 @@ static int queue_timestep(hst_ctx* ctx, double* time, double deltat);
 // as they were.  The report lists every candidate with its time a step.
 extern "C" int hst_gpu_autotune(hst_ctx* ctx, double deltat, int steps, char* report, int report_len) {
   if (!ctx || steps < 1) return fail(ctx, HST_EARG, "autotune: bad arguments");
+  if (ctx->nmem > 1) return fail(ctx, HST_EARG, "autotune: not for an ensemble context");
   CK(cudaSetDevice(ctx->device));
   Geometry& g = ctx->g;
   const Geometry g0 = g;
@@ -1183,21 +1258,24 @@ static int queue_timestep(hst_ctx* ctx, double* time, double deltat) {
                                   {120.0 / 20.0, 90.0 / 20.0, 50.0 / 20.0}};
   const hst_gpu_params& p = ctx->p;
   const bool damp = damping_active(p);
+  // every member of an ensemble at once (the base buffers); the field itself otherwise
+  const Geometry& G = ctx->nmem > 1 ? ctx->gb : ctx->g;
+  const DeviceState& D = ctx->nmem > 1 ? ctx->db : ctx->d;
   for (int i = 0; i < 3; ++i) {
     const double* ODE = RK[i];
     const double t = *time;
     if (!p.linear || i == 2) {
-      if (i == 2) CK(cudaMemsetAsync(ctx->d.cfl, 0, sizeof(unsigned long long), ctx->stream));
-      CK(timed(ctx, HST_KC_ZINV, [&] { return hst::launch_zinv(ctx->g, ctx->d, ctx->stream); }));
-      CK(timed(ctx, HST_KC_XPROD, [&] { return hst::launch_xprod(ctx->g, ctx->d, ctx->ps, i == 2, ctx->stream); }));
-      if (!p.linear) CK(timed(ctx, HST_KC_ZFWD, [&] { return hst::launch_zfwd(ctx->g, ctx->d, ctx->stream); }));
+      if (i == 2) CK(cudaMemsetAsync(D.cfl, 0, sizeof(unsigned long long), ctx->stream));
+      CK(timed(ctx, HST_KC_ZINV, [&] { return hst::launch_zinv(G, D, ctx->stream); }));
+      CK(timed(ctx, HST_KC_XPROD, [&] { return hst::launch_xprod(G, D, ctx->ps, i == 2, ctx->stream); }));
+      if (!p.linear) CK(timed(ctx, HST_KC_ZFWD, [&] { return hst::launch_zfwd(G, D, ctx->stream); }));
     }
     if (damp && damping_update(ctx, t)) {
       // stream-ordered upload of the new table (the previous copy has been
       // consumed once the stream reaches it, so wait before refilling)
       CK(cudaStreamSynchronize(ctx->stream));
       std::memcpy(ctx->h_gdamp, ctx->gdamp.data(), sizeof(double) * ctx->g.ncol);
-      CK(cudaMemcpyAsync(ctx->d.gdamp, ctx->h_gdamp, sizeof(double) * ctx->g.ncol, cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(D.gdamp, ctx->h_gdamp, sizeof(double) * ctx->g.ncol, cudaMemcpyHostToDevice, ctx->stream));
     }
     SubstepScalars sc;
     sc.ode0 = ODE[0];
@@ -1217,22 +1295,22 @@ static int queue_timestep(hst_ctx* ctx, double* time, double deltat) {
     shear_shifts(ctx, t + dt_sub, &sc.sx_n, &sc.sz_n);
     if (ctx->column_split) {
       CK(timed(ctx, HST_KC_RHS,
-               [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, 1, ctx->stream); }));
+               [&] { return hst::launch_column(G, D, ctx->ps, sc, p.exact_shift, !p.linear, 1, ctx->stream); }));
       if (p.exact_shift && ctx->shift_split) {
         // the exact_shift shift as a kernel of its own (two lines a group,
         // no factor scratch: more warps an SM), then the solves
         CK(timed(ctx, HST_KC_SHIFT,
-                 [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, 1, 0, 3, ctx->stream); }));
+                 [&] { return hst::launch_column(G, D, ctx->ps, sc, 1, 0, 3, ctx->stream); }));
         CK(timed(ctx, HST_KC_COLUMN,
-                 [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, 0, !p.linear, 2, ctx->stream); }));
+                 [&] { return hst::launch_column(G, D, ctx->ps, sc, 0, !p.linear, 2, ctx->stream); }));
       } else {
         CK(timed(ctx, HST_KC_COLUMN, [&] {
-          return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, 2, ctx->stream);
+          return hst::launch_column(G, D, ctx->ps, sc, p.exact_shift, !p.linear, 2, ctx->stream);
         }));
       }
     } else {
       CK(timed(ctx, HST_KC_COLUMN,
-               [&] { return hst::launch_column(ctx->g, ctx->d, ctx->ps, sc, p.exact_shift, !p.linear, 0, ctx->stream); }));
+               [&] { return hst::launch_column(G, D, ctx->ps, sc, p.exact_shift, !p.linear, 0, ctx->stream); }));
     }
     *time = t + dt_sub;
   }

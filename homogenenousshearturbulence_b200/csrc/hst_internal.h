@@ -26,6 +26,12 @@ struct Geometry {
   // 0, or (in the view of the four ghost rows that the edge transforms take)
   // ny: the z-inverse then reads rows -2, -1, ny, ny+1 of V
   int edge_gap;
+  // members of an ensemble advanced together (1 for a single field): every
+  // per-field buffer holds nmem members one after another (fields nf
+  // elements a member, Z 3 ny nzd nxB, Pp 6 ny nzd nxB, Q 6 ncol ny), the
+  // tables are shared, and the substep's kernels cover all members in one
+  // launch each
+  int nmem;
 };
 
 struct DeviceState {

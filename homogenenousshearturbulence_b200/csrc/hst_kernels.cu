@@ -88,9 +88,12 @@ enum { COL_FUSED = 0, COL_RHS = 1, COL_SOLVE = 2, COL_SHIFT = 3 };
 // back-substitution factors of the D2V and ETA solves, (m-2) x 4 x P
 // doubles, in shared or in global memory).
 template <int P, bool EXACT, bool NONLIN, int MODE>
-__device__ __forceinline__ void column_body(const ColumnArgs& a, int col, int s, cxd* bufA, cxd* bufB, cxd* bufC,
+__device__ __forceinline__ void column_body(const ColumnArgs& a, int cg, int s, cxd* bufA, cxd* bufB, cxd* bufC,
                                             double* fac) {
   const Geometry& g = a.g;
+  // cg: the column over all members (the fields' column index); col: the
+  // Fourier column within its member
+  const int mem = cg / g.ncol, col = cg - mem * g.ncol;
   const int ny = g.ny, nz = g.nz, nzT = g.nzT;
   LineGeom G;
   G.n = ny;
@@ -105,7 +108,7 @@ __device__ __forceinline__ void column_body(const ColumnArgs& a, int col, int s,
   const double kk = al * al + be * be;
   const double ni = a.ps.ni;
   const SubstepScalars sc = a.sc;
-  const size_t cb = (size_t)col * g.rows + 2;  // row 0 of the column
+  const size_t cb = (size_t)cg * g.rows + 2;  // row 0 of the column
   const double2* __restrict__ V1c = a.V1 + cb;
   const double2* __restrict__ V2c = a.V2 + cb;
   const double2* __restrict__ V3c = a.V3 + cb;
@@ -115,13 +118,14 @@ __device__ __forceinline__ void column_body(const ColumnArgs& a, int col, int s,
   // ---- right-hand sides, row by row (buildrhs_prepare :92-141, buildrhs :151-213)
   if (MODE == COL_FUSED || MODE == COL_RHS) {
     const ColConst cc = col_const(col, g, a.ps, sc, a.gdamp);
-    const double2* Qc = a.Q + (size_t)col * ny;
+    const double2* Qc = a.Q + ((size_t)mem * 6 * g.ncol + col) * ny;
     const size_t qs = (size_t)g.ncol * ny;
 #pragma unroll 1
     for (int r = s; r < ny; r += P) {
       auto tv = [&](int c, int j) -> cxd { return (c == 0 ? V1c : (c == 1 ? V2c : V3c))[r + j - 2]; };
       auto tq = [&](int p, int j) -> cxd {
-        return q_at(Qc + p * qs, a.Qg ? a.Qg + ((size_t)p * g.ncol + col) * 4 : nullptr, r + j - 2, ny, cc.ph_t);
+        return q_at(Qc + p * qs, a.Qg ? a.Qg + (((size_t)mem * 6 + p) * g.ncol + col) * 4 : nullptr, r + j - 2, ny,
+                    cc.ph_t);
       };
       const size_t ro = cb + r;
       cxd r1, r2, o1, o2;
@@ -149,11 +153,11 @@ __device__ __forceinline__ void column_body(const ColumnArgs& a, int col, int s,
   // that it holds two lines, not three; the pairs share the solves' table
   // loads and the phases.
   const double th0 = al * sc.sx_t + be * sc.sz_t;
-  double2* scr = a.V1 + (size_t)col * g.rows;
+  double2* scr = a.V1 + (size_t)cg * g.rows;
   if ((MODE == COL_SOLVE || MODE == COL_SHIFT) && EXACT) {
     const double gx = al * sc.dgx + be * sc.dgz;
     const cxd phs = cexpi(-(al * sc.sx_n + be * sc.sz_n));
-    double2* scr2 = a.V3 + (size_t)col * g.rows;
+    double2* scr2 = a.V3 + (size_t)cg * g.rows;
     cxd* const bufs[2] = {bufA, bufB};
 #pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
@@ -255,7 +259,7 @@ __device__ __forceinline__ void column_body(const ColumnArgs& a, int col, int s,
   __syncwarp(gmask);
   group_solve<P>(K_ETA, sc.lambda, ni, kk, thn, DS, G, bufA, fac, s, gmask);
   __syncwarp(gmask);
-  double2* V2w = a.V2 + (size_t)col * g.rows;
+  double2* V2w = a.V2 + (size_t)cg * g.rows;
   store_with_ghosts<P>(V2w, bufB, G, ny, phn, s, c00);
   __syncwarp(gmask);
   // D1 v through the ghost rows, then D0 (dv/dy) = D1 v (KIND_DY)
@@ -292,8 +296,8 @@ __device__ __forceinline__ void column_body(const ColumnArgs& a, int col, int s,
     bufB[G.at(r)] = w;
   }
   __syncwarp(gmask);
-  store_with_ghosts<P>(a.V1 + (size_t)col * g.rows, bufA, G, ny, phn, s, false);
-  store_with_ghosts<P>(a.V3 + (size_t)col * g.rows, bufB, G, ny, phn, s, false);
+  store_with_ghosts<P>(a.V1 + (size_t)cg * g.rows, bufA, G, ny, phn, s, false);
+  store_with_ghosts<P>(a.V3 + (size_t)cg * g.rows, bufB, G, ny, phn, s, false);
 }
 
 // The five-point stencil n (0: D0, 1: D1) of a line held slab by slab in
@@ -350,9 +354,10 @@ __device__ __forceinline__ void slab_stencil(int n, const SlabDer& DS, cxd* sb, 
 //   V2, D1 stencil of v and the DY solve (table) in place, u and w, V1 and
 //   V3 with their ghost rows.
 template <int P, bool EXACT, bool SHIFT_ONLY>
-__device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int col, int s, cxd* bufA, cxd* bufB,
+__device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, int s, cxd* bufA, cxd* bufB,
                                                   double* fac) {
   const Geometry& g = a.g;
+  const int mem = cg / g.ncol, col = cg - mem * g.ncol;
   const int ny = g.ny, nz = g.nz, nzT = g.nzT, m = g.m;
   LineGeom G;
   G.n = ny;
@@ -366,7 +371,7 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int col, 
   const double al = a.ps.alfa0 * ix, be = a.ps.beta0 * iz;
   const double kk = al * al + be * be;
   const SubstepScalars& sc = a.sc;
-  const size_t cb = (size_t)col * g.rows + 2;  // row 0 of the column
+  const size_t cb = (size_t)cg * g.rows + 2;  // row 0 of the column
   const SlabDer DS = {a.derS, m, P};
   cxd* const sA = bufA + s * G.MS;  // this lane's slab
   cxd* const sB = bufB + s * G.MS;
@@ -424,7 +429,7 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int col, 
   __syncwarp(gmask);
   group_solve<P>(K_ETA, sc.lambda, a.ps.ni, kk, thn, DS, G, bufA, fac, s, gmask);
   __syncwarp(gmask);
-  store_with_ghosts<P>(a.V2 + (size_t)col * g.rows, bufB, G, ny, phn, s, c00);
+  store_with_ghosts<P>(a.V2 + (size_t)cg * g.rows, bufB, G, ny, phn, s, c00);
   // D1 v through the ghost rows, then D0 (dv/dy) = D1 v (KIND_DY); the (0,0)
   // column's v is zero
   if (c00)
@@ -454,8 +459,8 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int col, 
     sB[i] = w;
   }
   __syncwarp(gmask);
-  store_with_ghosts<P>(a.V1 + (size_t)col * g.rows, bufA, G, ny, phn, s, false);
-  store_with_ghosts<P>(a.V3 + (size_t)col * g.rows, bufB, G, ny, phn, s, false);
+  store_with_ghosts<P>(a.V1 + (size_t)cg * g.rows, bufA, G, ny, phn, s, false);
+  store_with_ghosts<P>(a.V3 + (size_t)cg * g.rows, bufB, G, ny, phn, s, false);
 }
 
 // One group of P lanes per Fourier column, every intermediate in shared
@@ -468,8 +473,8 @@ __global__ void k_column(ColumnArgs a) {
   const Geometry& g = a.g;
   const int groups = blockDim.x / P;
   const int grp = threadIdx.x / P, s = threadIdx.x - grp * P;
-  const int col = blockIdx.x * groups + grp;
-  if (col >= g.ncol) return;
+  const int col = blockIdx.x * groups + grp;  // over all members
+  if (col >= g.ncol * g.nmem) return;
   const int mi = g.m - 2;
   const int lineN = P * g.MS;
   constexpr int NL = (EXACT && MODE == COL_FUSED) ? 3 : 2;  // lines held
@@ -504,7 +509,7 @@ __global__ void __launch_bounds__(64, COLSOLVE_MINB) k_column_solve(ColumnArgs a
   const int slot = blockIdx.x * groups + grp;
   // the factor scratch: the group's slice of a.facg, or after its lines
   double* fac = a.facg ? a.facg + (size_t)slot * facn : reinterpret_cast<double*>(bufB + lineN);
-  for (int col = slot; col < g.ncol; col += gridDim.x * groups)
+  for (int col = slot; col < g.ncol * g.nmem; col += gridDim.x * groups)
     column_solve_body<P, EXACT, SHIFT_ONLY>(a, col, s, bufA, bufB, fac);
 }
 
@@ -601,8 +606,9 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
   const Geometry& g = a.g;
   const int ny = g.ny;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int col = blockIdx.x * RT_WARPS + warp;
-  if (col >= g.ncol) return;
+  const int cgl = blockIdx.x * RT_WARPS + warp;  // the column over all members
+  if (cgl >= g.ncol * g.nmem) return;
+  const int mem = cgl / g.ncol, col = cgl - mem * g.ncol;
   double2* st0 = smt + (size_t)warp * 2 * RT_STAGE;
   uint64_t* bar = bars[warp];
   if (lane == 0) {
@@ -612,7 +618,7 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
   }
   __syncwarp();
   const int ntile = ny / 32;
-  const size_t cbase = (size_t)col * g.rows;  // row -2 of the column
+  const size_t cbase = (size_t)cgl * g.rows;  // row -2 of the column
   const double2* Vg[3] = {a.V1, a.V2, a.V3};
   // lane 0 queues the copies of tile t into stage t & 1
   const QT* Qg = reinterpret_cast<const QT*>(a.Q);
@@ -627,13 +633,13 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
     for (int c = 0; c < 3; ++c) bulk_g2s(S + c * RT_W, Vg[c] + cbase + r0, RT_W * 16, &bar[stg]);
 #pragma unroll 1
     for (int p = 0; p < 6; ++p) {
-      const QT* Qc = Qg + ((size_t)p * g.ncol + col) * ny;
+      const QT* Qc = Qg + (((size_t)mem * 6 + p) * g.ncol + col) * ny;
       QT* D = reinterpret_cast<QT*>(S + 3 * RT_W) + p * RT_W;
       const int lo = r0 - 2, hi = r0 + 34;
       const int m0 = lo < 0 ? 0 : lo, m1 = hi > ny ? ny : hi;
       // the rows beyond the box: the wrapped interior rows (their phase is
       // applied in tq), or the ghost rows' own spectra
-      const QT* Qgc = Qgg ? Qgg + ((size_t)p * g.ncol + col) * 4 : nullptr;
+      const QT* Qgc = Qgg ? Qgg + (((size_t)mem * 6 + p) * g.ncol + col) * 4 : nullptr;
       if (lo < 0) bulk_g2s(D, Qgc ? Qgc : Qc + ny + lo, (unsigned)(-lo) * QE, &bar[stg]);
       bulk_g2s(D + (m0 - lo), Qc + m0, (unsigned)(m1 - m0) * QE, &bar[stg]);
       if (hi > ny) bulk_g2s(D + (ny - lo), Qgc ? Qgc + 2 : Qc, (unsigned)(hi - ny) * QE, &bar[stg]);
@@ -720,7 +726,7 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
   const Geometry& g = a.g;
   if (MODE == COL_RHS && g.ny % 32 == 0 && a.tiled) {  // TMA-staged tiles
     const size_t smem = (size_t)RT_WARPS * 2 * RT_STAGE * sizeof(double2);
-    const int blocks = (g.ncol + RT_WARPS - 1) / RT_WARPS;
+    const int blocks = (g.ncol * g.nmem + RT_WARPS - 1) / RT_WARPS;
     if (g.mp) {
       smem_limit(*a.dstate, k_rhs_tiled<EXACT, NONLIN, float2>, (int)smem);
       k_rhs_tiled<EXACT, NONLIN, float2><<<blocks, 32 * RT_WARPS, smem, st>>>(a, a.err);
@@ -734,7 +740,7 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
   // linear right-hand sides read none)
   if (MODE != COL_SOLVE && MODE != COL_SHIFT && g.mp && NONLIN) return cudaErrorInvalidValue;
   if (MODE == COL_RHS) {  // one warp per column, four per block, no shared memory
-    const int blocks = (g.ncol + 3) / 4;
+    const int blocks = (g.ncol * g.nmem + 3) / 4;
     k_column<32, EXACT, NONLIN, COL_RHS><<<blocks, 128, 0, st>>>(a);
     return cudaGetLastError();
   }
@@ -752,7 +758,7 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
   if (per * groups > 200 * 1024) return cudaErrorInvalidValue;
   const int T = groups * P;
   size_t smem = per * groups;
-  int blocks = (g.ncol + groups - 1) / groups;
+  int blocks = (g.ncol * g.nmem + groups - 1) / groups;
   if (gfac) {
     auto kern = k_column_solve<P, EXACT, MODE == COL_SHIFT>;
     smem_limit(*a.dstate, kern, 200 * 1024);

@@ -80,16 +80,20 @@ __device__ __forceinline__ void zinv_body(const Geometry& g, const double2* __re
                                           C* __restrict__ Z, const C* __restrict__ twz) {
   extern __shared__ double2 sh_d[];
   C* sh = reinterpret_cast<C*>(sh_d);
-  const int yt = blockIdx.x, ix = blockIdx.y, c = blockIdx.z;
+  const int yt = blockIdx.x, ix = blockIdx.y, c = blockIdx.z % 3, mem = blockIdx.z / 3;
   const int Ty = g.Ty, NZ = g.nzd, nyT = g.ny / Ty;
-  const double2* V = c == 0 ? V0 : (c == 1 ? V1 : V2);
+  const double2* V = (c == 0 ? V0 : (c == 1 ? V1 : V2)) + (size_t)mem * g.nf;
+  Z += (size_t)mem * 3 * NZ * g.ny * g.nxB;
   const ZinvSrc<C> src = {V + (size_t)ix * g.nzT * g.rows + (g.edge_gap ? 0 : 2) + yt * Ty, g.rows, g.nz, NZ,
                           g.edge_gap};
   const TileDst<C> dst = {Z + (((size_t)c * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
   fft_sel<NT, +1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
 }
 template <int NT, int PPT, typename C>
-__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256) k_zinv(Geometry g, const double2* __restrict__ V0,
+#ifndef ZT768
+#define ZT768 0
+#endif
+__global__ void __launch_bounds__(PPT <= 8 ? (ZT768 ? 768 : 512) : 256) k_zinv(Geometry g, const double2* __restrict__ V0,
                                               const double2* __restrict__ V1, const double2* __restrict__ V2,
                                               C* __restrict__ Z, const C* __restrict__ twz) {
   zinv_body<NT, PPT, C>(g, V0, V1, V2, Z, twz);
@@ -123,12 +127,14 @@ struct ZfwdDst {
 // 256; the same on k_zinv measured slower; the 8-point plans are held to
 // two blocks an SM)
 template <int NT, int PPT, typename C>
-__global__ void __launch_bounds__(PPT <= 8 ? 384 : 256, PPT <= 8 ? 2 : 1) k_zfwd(Geometry g, const C* __restrict__ Pp, C* __restrict__ Q,
+__global__ void __launch_bounds__(PPT <= 8 ? (ZT768 ? 768 : 384) : 256, PPT <= 8 && !ZT768 ? 2 : 1) k_zfwd(Geometry g, const C* __restrict__ Pp, C* __restrict__ Q,
                                               const C* __restrict__ twz) {
   extern __shared__ double2 sh_d[];
   C* sh = reinterpret_cast<C*>(sh_d);
-  const int yt = blockIdx.x, ix = blockIdx.y, p = blockIdx.z;
+  const int yt = blockIdx.x, ix = blockIdx.y, p = blockIdx.z % 6, mem = blockIdx.z / 6;
   const int Ty = g.Ty, NZ = g.nzd, nyT = g.ny / Ty;
+  Pp += (size_t)mem * 6 * NZ * g.ny * g.nxB;
+  Q += (size_t)mem * 6 * g.ncol * g.ny;
   const TileSrc<C> src = {Pp + (((size_t)p * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
   const ZfwdDst<C> dst = {Q + ((size_t)p * g.ncol + (size_t)ix * g.nzT) * g.ny + yt * Ty, g.ny, g.nz, NZ};
   fft_sel<NT, -1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
@@ -259,7 +265,9 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   using LT = std::conditional_t<JF, ShLinesPT<C>, ShLinesT<C>>;
   const int NX = 2 * g.nxd, nx = g.nx, nxB = g.nxB, NZ = g.nzd, Ty = g.Ty, LS = JF ? ls_padded(NX) : NX + 1;
   const int nyT = g.ny / Ty;
-  const int y0 = 2 * blockIdx.x, kz = blockIdx.y;
+  const int y0 = 2 * blockIdx.x, kz = blockIdx.y % g.nzd, mem = blockIdx.y / g.nzd;
+  Z += (size_t)mem * 3 * g.nzd * g.ny * g.nxB;
+  Pp += (size_t)mem * 6 * g.nzd * g.ny * g.nxB;
   const int yt = y0 / Ty, yi0 = y0 - yt * Ty;
   const size_t cs = (size_t)NZ * nyT * nxB * Ty;
   const size_t tile = ((size_t)yt * NZ + kz) * nxB * Ty;
@@ -283,7 +291,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
       mbar_init(bar, 1);
       fence_mbar_init();
       mbar_arrive_expect_tx(bar, 3u * nxB * 2u * (unsigned)sizeof(C));
-      tma_load_4d(stg, &tmZ, 2 * yi0, 0, yt * NZ + kz, 0, bar);
+      tma_load_4d(stg, &tmZ, 2 * yi0, 0, yt * NZ + kz, 3 * mem, bar);
       bool ok = mbar_wait_bounded(bar, 0, XPROD_WAIT_LIMIT);
       if (!ok) {
         // record the failure and give the copy a second bounded wait
@@ -378,7 +386,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
     fence_proxy_async();
     __syncthreads();
     if (threadIdx.x == 0) {
-      tma_store_4d(&tmP, 2 * yi0, 0, yt * NZ + kz, 0, stg_out);
+      tma_store_4d(&tmP, 2 * yi0, 0, yt * NZ + kz, 6 * mem, stg_out);
       bulk_commit();
       bulk_wait_read_all();
     }
@@ -532,7 +540,7 @@ cudaError_t make_transform_maps(const Geometry& g, DeviceState& d) {
   const int nyT = g.ny / g.Ty;
   for (int which = 0; which < 2; ++which) {
     const cuuint32_t comps = which == 0 ? 3 : 6;
-    cuuint64_t dims[4] = {(cuuint64_t)2 * g.Ty, (cuuint64_t)g.nxB, (cuuint64_t)g.nzd * nyT, comps};
+    cuuint64_t dims[4] = {(cuuint64_t)2 * g.Ty, (cuuint64_t)g.nxB, (cuuint64_t)g.nzd * nyT, (cuuint64_t)comps * g.nmem};
     const cuuint64_t es = g.mp ? 8 : 16;  // bytes of one complex element
     cuuint64_t strides[3] = {es * g.Ty, es * g.Ty * g.nxB, es * g.Ty * g.nxB * g.nzd * nyT};
     cuuint32_t box[4] = {4, (cuuint32_t)g.nxB, 1, comps};
@@ -542,7 +550,7 @@ cudaError_t make_transform_maps(const Geometry& g, DeviceState& d) {
                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
     if (d.Zg) {  // the ghost rows' buffers: one tile of four rows
-      cuuint64_t dg[4] = {8, (cuuint64_t)g.nxB, (cuuint64_t)g.nzd, comps};
+      cuuint64_t dg[4] = {8, (cuuint64_t)g.nxB, (cuuint64_t)g.nzd, (cuuint64_t)comps * g.nmem};
       cuuint64_t sg[3] = {es * 4, es * 4 * g.nxB, es * 4 * g.nxB * g.nzd};
       r = enc(which == 0 ? &d.tmZg : &d.tmPpg, g.mp ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
               which == 0 ? (void*)d.Zg : (void*)d.Ppg, dg, sg, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -628,7 +636,7 @@ bool mp_length_ok(int n) { return n == 96 || n == 192 || n == 384 || n == 768 ||
 
 static cudaError_t launch_zinv_main(const Geometry& g, const DeviceState& d, cudaStream_t st) {
   const int pts = g.nzd * g.Ty;
-  const dim3 grid(g.ny / g.Ty, g.nxB, 3);
+  const dim3 grid(g.ny / g.Ty, g.nxB, 3 * g.nmem);
   if (g.mp) {
     typedef float2 C;
     const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
@@ -661,7 +669,7 @@ static cudaError_t launch_zinv_main(const Geometry& g, const DeviceState& d, cud
 
 static cudaError_t launch_zfwd_main(const Geometry& g, const DeviceState& d, cudaStream_t st) {
   const int pts = g.nzd * g.Ty;
-  const dim3 grid(g.ny / g.Ty, g.nxB, 6);
+  const dim3 grid(g.ny / g.Ty, g.nxB, 6 * g.nmem);
   if (g.mp) {
     typedef float2 C;
     const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
@@ -693,7 +701,7 @@ static cudaError_t launch_xprod_main(const Geometry& g, const DeviceState& d, co
   const int NX = 2 * g.nxd;
   const int pts = 6 * NX;
   if (xprod_uses_maps(g) != d.maps) return cudaErrorInvalidValue;
-  const dim3 grid(g.ny / 2, g.nzd);
+  const dim3 grid(g.ny / 2, g.nzd * g.nmem);
   if (g.mp) {
     typedef float2 C;
     const size_t smem = !xprod_uses_maps(g) ? (size_t)6 * (NX + 1) * sizeof(C)

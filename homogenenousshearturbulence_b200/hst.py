@@ -88,6 +88,9 @@ def lib():
         d, i, vp = ct.c_double, ct.c_int, ct.c_void_p
         sig = {
             "hst_gpu_create": (i, [P(Params), P(vp)]),
+            "hst_gpu_create_batch": (i, [P(Params), i, P(vp)]),
+            "hst_gpu_select_member": (i, [vp, i]),
+            "hst_gpu_members": (i, [vp]),
             "hst_gpu_destroy": (i, [vp]),
             "hst_gpu_last_error": (ct.c_char_p, [vp]),
             "hst_gpu_device_bytes": (d, [P(Params)]),
@@ -229,9 +232,12 @@ def padded_sizes(nx, nz, nxd=0, nzd=0):
 
 # --------------------------------------------------------------- solver ----
 class Solver:
-    """One field resident on one GPU (one hst_ctx)."""
+    """One field resident on one GPU (one hst_ctx); with members > 1 an
+    ensemble of independent realisations of the deck advanced together
+    (hst_gpu_create_batch): timestep() runs every member, and the field calls
+    act on the member chosen with select()."""
 
-    def __init__(self, deck: dict | None = None, device: int = 0, **kw):
+    def __init__(self, deck: dict | None = None, device: int = 0, members: int = 1, **kw):
         cfg = dict(DECK_DEFAULTS)
         if deck:
             cfg.update(deck)
@@ -256,7 +262,11 @@ class Solver:
         p.precision = {"fp64": PREC_FP64, "mixed": PREC_MIXED}.get(prec, prec) if isinstance(prec, str) else int(prec)
         self.params = p
         self._h = ct.c_void_p()
-        rc = lib().hst_gpu_create(ct.byref(p), ct.byref(self._h))
+        self.members = int(members)
+        if self.members > 1:
+            rc = lib().hst_gpu_create_batch(ct.byref(p), self.members, ct.byref(self._h))
+        else:
+            rc = lib().hst_gpu_create(ct.byref(p), ct.byref(self._h))
         if rc != 0:
             raise HstError(f"hst_gpu_create failed ({rc}) for nx={p.nx} ny={p.ny} nz={p.nz}", rc)
         self.nx, self.ny, self.nz = p.nx, p.ny, p.nz
@@ -277,6 +287,10 @@ class Solver:
         self.der = der.reshape(5, 4, ny)  # der[j+2, n, iy] = der(iy, n, j)
         self.y = y
         self.dyl = dyl
+
+    def select(self, member: int):
+        """the member the field calls act on (an ensemble context)"""
+        self._check(lib().hst_gpu_select_member(self._h, int(member)), "select_member")
 
     def close(self):
         if self._h:

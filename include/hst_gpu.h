@@ -97,6 +97,19 @@ typedef struct hst_ctx hst_ctx;
  * damping_setup do (src/hst_setup.f90:42-71, src/hst_derivatives.f90:30-56,
  * src/hst_damping.f90:68-78), uploads them.  The fields start at zero. */
 int hst_gpu_create(const hst_gpu_params* p, hst_ctx** out);
+/* An ensemble: nmem independent realisations of the same deck (same sizes,
+ * physics, time step; their own initial fields) in one context, advanced
+ * together -- hst_gpu_timestep / _timesteps run every member, each kernel
+ * of the substep covering all members in one launch, and the CFL number is
+ * the largest over the members.  The per-field device memory is nmem times
+ * that of a single field; the tables are shared.  Every other entry point
+ * (upload, download, fill_ghosts, line_solve, outstats, pressure, restart
+ * files, the pieces, the asynchronous I/O) acts on the member chosen by
+ * hst_gpu_select_member (member 0 at first).  hst_gpu_autotune refuses an
+ * ensemble.  No counterpart in the reference, which runs one field a job. */
+int hst_gpu_create_batch(const hst_gpu_params* p, int nmem, hst_ctx** out);
+int hst_gpu_select_member(hst_ctx* ctx, int member);
+int hst_gpu_members(const hst_ctx* ctx);
 int hst_gpu_destroy(hst_ctx* ctx);
 const char* hst_gpu_last_error(const hst_ctx* ctx);
 /* Device bytes held by a context of these sizes (0 on bad sizes). */
