@@ -353,6 +353,9 @@ __device__ __forceinline__ void slab_stencil(int n, const SlabDer& DS, cxd* sb, 
 //   then linsolve (:298-326): D2V and ETA solves, v with its ghost rows to
 //   V2, D1 stencil of v and the DY solve (table) in place, u and w, V1 and
 //   V3 with their ghost rows.
+#ifndef HST_SHIFT_PAIRS
+#define HST_SHIFT_PAIRS 0
+#endif
 template <int P, bool EXACT, bool SHIFT_ONLY>
 __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, int s, cxd* bufA, cxd* bufB,
                                                   double* fac) {
@@ -384,6 +387,45 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, i
     // rows follow by one complex product each (dy = ly / ny apart)
     const cxd e0 = cexpi(-gx * a.y[s * m + 2]);
     const cxd estep = sc.yuni ? cexpi(-gx * (sc.ytile / 32.0)) : mkc(1.0, 0.0);
+#if HST_SHIFT_PAIRS
+    // two lines a pass (old1 with old2, then rhs1 with rhs2): the solves
+    // share the table loads and run as two independent chains
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+      const double2* s1 = pass == 0 ? a.O1 : a.R1;
+      const double2* s2 = pass == 0 ? a.O2 : a.R2;
+      for (int r = s; r < ny; r += P) {
+        bufA[G.at(r)] = s1[cb + r];
+        bufB[G.at(r)] = s2[cb + r];
+      }
+      __syncwarp(gmask);
+      {
+        cxd* const bufs[2] = {bufA, bufB};
+        group_solve_d0<P, 2>(th0, a.d0tab, G, bufs, s, gmask);
+      }
+      __syncwarp(gmask);
+      cxd e = e0;
+      for (int i = 0; i < m; ++i) {
+        if (!sc.yuni && i > 0) e = cexpi(-gx * a.y[s * m + i + 2]);
+        sA[i] = cmul(sA[i], e);
+        sB[i] = cmul(sB[i], e);
+        e = cmul(e, estep);
+      }
+      __syncwarp(gmask);
+      slab_stencil<P>(0, DS, sA, m, s, phs, gmask);
+      slab_stencil<P>(0, DS, sB, m, s, phs, gmask);
+      __syncwarp(gmask);
+      if (pass == 0 || SHIFT_ONLY) {
+        double2* d1 = pass == 0 ? a.O1 : a.R1;
+        double2* d2 = pass == 0 ? a.O2 : a.R2;
+        for (int r = s; r < ny; r += P) {
+          d1[cb + r] = bufA[G.at(r)];
+          d2[cb + r] = bufB[G.at(r)];
+        }
+        __syncwarp(gmask);
+      }
+    }
+#else
 #pragma unroll 1
     for (int q = 0; q < 4; ++q) {
       // q = 0, 1: old1, old2 (back to OLD1, OLD2 through bufA); 2: rhs1
@@ -413,6 +455,7 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, i
         __syncwarp(gmask);
       }
     }
+#endif
     if (SHIFT_ONLY) return;
   } else {
     for (int r = s; r < ny; r += P) {
