@@ -162,6 +162,7 @@ struct hst_ctx {
   // 4.4 + solves 4.9 ms against 10.3 ms in one kernel), HST_SHIFT_SPLIT=0 / 1
   // forces it
   bool shift_split;
+  bool solve_halves;  // the solve stage as two one-line passes
   // per-kernel-class CUDA-event accounting (hst_gpu_set_profiling)
   bool prof_on;
   std::vector<cudaEvent_t> ev;
@@ -193,7 +194,7 @@ struct hst_ctx {
 // Runs `launch` (which queues one kernel on ctx->stream) between two events
 // when profiling is on, and counts it.
 template <typename F>
-static cudaError_t timed(hst_ctx* c, int kc, F launch) {
+static cudaError_t timed(hst_ctx* c, int kc, F launch, int nlaunch = 1) {
   cudaEvent_t a = nullptr, b = nullptr;
   if (c->prof_on) {
     size_t k = c->ev_class.size();
@@ -209,7 +210,7 @@ static cudaError_t timed(hst_ctx* c, int kc, F launch) {
   }
   cudaError_t r = launch();
   if (r != cudaSuccess) return r;
-  c->launches++;
+  c->launches += nlaunch;
   if (c->prof_on) {
     cudaEventRecord(b, c->stream);
     c->ev_class.push_back(kc);
@@ -287,10 +288,6 @@ static bool damping_update(hst_ctx* c, double t) {
 }
 
 // ------------------------------------------------------ geometry ----
-#ifndef ZT768
-#define ZT768 0
-#endif
-#define ZT_MAX_THREADS (ZT768 ? 768 : 384)
 static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& why) {
   g.nx = p.nx;
   g.ny = p.ny;
@@ -384,7 +381,7 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
   // transform y tile (at most 512 threads for the 8-point z plans)
   g.Ty = 2;
   for (int t : {8, 4}) {
-    if (p.ny % t == 0 && (size_t)t * (g.nzd + 1) * 16 <= 100 * 1024 && (g.pptz != 8 || t * g.nzd / 8 <= ZT_MAX_THREADS)) {
+    if (p.ny % t == 0 && (size_t)t * (g.nzd + 1) * 16 <= 100 * 1024 && (g.pptz != 8 || t * g.nzd / 8 <= 384)) {
       g.Ty = t;
       break;
     }
@@ -509,6 +506,7 @@ static int create_context(const hst_gpu_params* pin, int nmem, hst_ctx** out) {
     const char* e = std::getenv("HST_COLUMN_FUSED");
     ctx->column_split = !(e && std::atoi(e) == 1);
     ctx->shift_split = false;  // decided once the geometry is known
+    ctx->solve_halves = false;
   }
   ctx->prof_on = false;
   for (int k = 0; k < HST_KC_N; ++k) {
@@ -667,6 +665,9 @@ static int create_context(const hst_gpu_params* pin, int nmem, hst_ctx** out) {
   {
     const char* f = std::getenv("HST_SHIFT_SPLIT");
     ctx->shift_split = f ? std::atoi(f) == 1 : ctx->d.facg != nullptr;
+    // the solves in two one-line passes (needs the global factor scratch)
+    const char* h = std::getenv("HST_SOLVE_HALVES");
+    ctx->solve_halves = ctx->d.facg != nullptr && (h ? std::atoi(h) == 1 : true);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -1252,6 +1253,21 @@ extern "C" int hst_gpu_read_restart(hst_ctx* ctx, const char* path, double* time
   return HST_OK;
 }
 
+// the solve stage of a substep whose right-hand sides (and exact_shift
+// shift) are done: one kernel, or its two one-line halves
+static cudaError_t solve_stage(hst_ctx* ctx, const hst::Geometry& G, const hst::DeviceState& D,
+                               const hst::SubstepScalars& sc, int nonlin) {
+  if (ctx->solve_halves)
+    return timed(
+        ctx, HST_KC_COLUMN,
+        [&] {
+          cudaError_t e = hst::launch_column(G, D, ctx->ps, sc, 0, nonlin, 5, ctx->stream);
+          return e == cudaSuccess ? hst::launch_column(G, D, ctx->ps, sc, 0, nonlin, 6, ctx->stream) : e;
+        },
+        2);
+  return timed(ctx, HST_KC_COLUMN, [&] { return hst::launch_column(G, D, ctx->ps, sc, 0, nonlin, 2, ctx->stream); });
+}
+
 // One time step (src/hst_equations.f90:56-87) queued on the stream.
 static int queue_timestep(hst_ctx* ctx, double* time, double deltat) {
   static const double RK[3][3] = {{120.0 / 32.0, 2.0, 0.0}, {120.0 / 8.0, 50.0 / 8.0, 34.0 / 8.0},
@@ -1297,12 +1313,13 @@ static int queue_timestep(hst_ctx* ctx, double* time, double deltat) {
       CK(timed(ctx, HST_KC_RHS,
                [&] { return hst::launch_column(G, D, ctx->ps, sc, p.exact_shift, !p.linear, 1, ctx->stream); }));
       if (p.exact_shift && ctx->shift_split) {
-        // the exact_shift shift as a kernel of its own (two lines a group,
+        // the exact_shift shift as a kernel of its own (one line a group,
         // no factor scratch: more warps an SM), then the solves
         CK(timed(ctx, HST_KC_SHIFT,
                  [&] { return hst::launch_column(G, D, ctx->ps, sc, 1, 0, 3, ctx->stream); }));
-        CK(timed(ctx, HST_KC_COLUMN,
-                 [&] { return hst::launch_column(G, D, ctx->ps, sc, 0, !p.linear, 2, ctx->stream); }));
+        CK(solve_stage(ctx, G, D, sc, !p.linear));
+      } else if (!p.exact_shift && ctx->solve_halves) {
+        CK(solve_stage(ctx, G, D, sc, !p.linear));
       } else {
         CK(timed(ctx, HST_KC_COLUMN, [&] {
           return hst::launch_column(G, D, ctx->ps, sc, p.exact_shift, !p.linear, 2, ctx->stream);

@@ -82,6 +82,9 @@ __device__ __forceinline__ void store_with_ghosts(double2* __restrict__ col, con
 // MODE 3 (EXACT only): the exact_shift shear shift of RHS1/2 and OLD1/2 in
 // place and nothing else (the per-piece shear_shift).
 enum { COL_FUSED = 0, COL_RHS = 1, COL_SOLVE = 2, COL_SHIFT = 3 };
+// MODE 5, 6: the solves of MODE 2 in two passes of one line each (the v
+// half, then the eta half with u and w), for the persistent form only
+enum { COL_SOLVE_V = 5, COL_SOLVE_ETA = 6 };
 
 // The work on one Fourier column (the body of k_column): bufA, bufB (bufC)
 // the group's line buffers in shared memory, fac its factor scratch (the
@@ -353,9 +356,6 @@ __device__ __forceinline__ void slab_stencil(int n, const SlabDer& DS, cxd* sb, 
 //   then linsolve (:298-326): D2V and ETA solves, v with its ghost rows to
 //   V2, D1 stencil of v and the DY solve (table) in place, u and w, V1 and
 //   V3 with their ghost rows.
-#ifndef HST_SHIFT_PAIRS
-#define HST_SHIFT_PAIRS 0
-#endif
 template <int P, bool EXACT, bool SHIFT_ONLY>
 __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, int s, cxd* bufA, cxd* bufB,
                                                   double* fac) {
@@ -387,51 +387,13 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, i
     // rows follow by one complex product each (dy = ly / ny apart)
     const cxd e0 = cexpi(-gx * a.y[s * m + 2]);
     const cxd estep = sc.yuni ? cexpi(-gx * (sc.ytile / 32.0)) : mkc(1.0, 0.0);
-#if HST_SHIFT_PAIRS
-    // two lines a pass (old1 with old2, then rhs1 with rhs2): the solves
-    // share the table loads and run as two independent chains
-#pragma unroll 1
-    for (int pass = 0; pass < 2; ++pass) {
-      const double2* s1 = pass == 0 ? a.O1 : a.R1;
-      const double2* s2 = pass == 0 ? a.O2 : a.R2;
-      for (int r = s; r < ny; r += P) {
-        bufA[G.at(r)] = s1[cb + r];
-        bufB[G.at(r)] = s2[cb + r];
-      }
-      __syncwarp(gmask);
-      {
-        cxd* const bufs[2] = {bufA, bufB};
-        group_solve_d0<P, 2>(th0, a.d0tab, G, bufs, s, gmask);
-      }
-      __syncwarp(gmask);
-      cxd e = e0;
-      for (int i = 0; i < m; ++i) {
-        if (!sc.yuni && i > 0) e = cexpi(-gx * a.y[s * m + i + 2]);
-        sA[i] = cmul(sA[i], e);
-        sB[i] = cmul(sB[i], e);
-        e = cmul(e, estep);
-      }
-      __syncwarp(gmask);
-      slab_stencil<P>(0, DS, sA, m, s, phs, gmask);
-      slab_stencil<P>(0, DS, sB, m, s, phs, gmask);
-      __syncwarp(gmask);
-      if (pass == 0 || SHIFT_ONLY) {
-        double2* d1 = pass == 0 ? a.O1 : a.R1;
-        double2* d2 = pass == 0 ? a.O2 : a.R2;
-        for (int r = s; r < ny; r += P) {
-          d1[cb + r] = bufA[G.at(r)];
-          d2[cb + r] = bufB[G.at(r)];
-        }
-        __syncwarp(gmask);
-      }
-    }
-#else
 #pragma unroll 1
     for (int q = 0; q < 4; ++q) {
       // q = 0, 1: old1, old2 (back to OLD1, OLD2 through bufA); 2: rhs1
-      // (kept in bufA); 3: rhs2 (kept in bufB)
-      cxd* X = q == 3 ? bufB : bufA;
-      cxd* sX = q == 3 ? sB : sA;
+      // (kept in bufA); 3: rhs2 (kept in bufB; the shift alone stores each
+      // line before it loads the next, all through bufA)
+      cxd* X = q == 3 && !SHIFT_ONLY ? bufB : bufA;
+      cxd* sX = q == 3 && !SHIFT_ONLY ? sB : sA;
       const double2* src = q == 0 ? a.O1 : (q == 1 ? a.O2 : (q == 2 ? a.R1 : a.R2));
       for (int r = s; r < ny; r += P) X[G.at(r)] = src[cb + r];
       __syncwarp(gmask);
@@ -455,7 +417,6 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, i
         __syncwarp(gmask);
       }
     }
-#endif
     if (SHIFT_ONLY) return;
   } else {
     for (int r = s; r < ny; r += P) {
@@ -529,13 +490,96 @@ __global__ void k_column(ColumnArgs a) {
   column_body<P, EXACT, NONLIN, MODE>(a, col, s, bufA, bufB, bufC, base + (size_t)NL * lineN * 2);
 }
 
-// The solve stage (SHIFT_ONLY: the exact_shift shift alone) on a persistent
-// grid: each group of P lanes walks the columns col, col + gridDim.x groups,
-// ...; shared memory holds only the group's two lines, and the group's
-// factor scratch is its own slice of a.facg in global memory, rewritten
-// column after column (so it stays in L2).  Fewer bytes of shared memory a
-// warp let more warps share an SM.
-template <int P, bool EXACT, bool SHIFT_ONLY>
+// The solves of column_solve_body in two passes of one line each, so that a
+// group holds one line of shared memory: HALF 0 solves D2V for v (V2 with
+// its ghost rows), takes D1 v and solves DY for dv/dy, which it leaves in
+// V1's interior rows; HALF 1 solves ETA, reads dv/dy back row by row and
+// writes u over it (then u's ghost rows) and w (V3 with its ghost rows).
+// The same operations in the same order as the one-pass form, so the same
+// bits.
+template <int P, int HALF>
+__device__ __forceinline__ void column_solve_half(const ColumnArgs& a, int cg, int s, cxd* buf, double* fac) {
+  const Geometry& g = a.g;
+  const int mem = cg / g.ncol, col = cg - mem * g.ncol;
+  const int ny = g.ny, nz = g.nz, nzT = g.nzT, m = g.m;
+  LineGeom G;
+  G.n = ny;
+  G.m = m;
+  G.MS = g.MS;
+  G.P = P;
+  G.invm = (unsigned)((1u << 20) + m - 1) / (unsigned)m;
+  const unsigned gmask = group_mask(P);
+  const int ix = col / nzT, iz = col - ix * nzT - nz;
+  const bool c00 = (ix == 0 && iz == 0);
+  const double al = a.ps.alfa0 * ix, be = a.ps.beta0 * iz;
+  const double kk = al * al + be * be;
+  const SubstepScalars& sc = a.sc;
+  const size_t cb = (size_t)cg * g.rows + 2;  // row 0 of the column
+  const SlabDer DS = {a.derS, m, P};
+  cxd* const sb = buf + s * G.MS;
+  const double thn = al * sc.sx_n + be * sc.sz_n;
+  const cxd phn = cexpi(-thn);
+  double2* const v1 = a.V1 + (size_t)cg * g.rows;
+  if (HALF == 0) {
+    for (int r = s; r < ny; r += P) buf[G.at(r)] = a.R2[cb + r];
+    __syncwarp(gmask);
+    group_solve<P>(K_D2V, sc.lambda, a.ps.ni, kk, thn, DS, G, buf, fac, s, gmask);
+    __syncwarp(gmask);
+    store_with_ghosts<P>(a.V2 + (size_t)cg * g.rows, buf, G, ny, phn, s, c00);
+    if (c00)
+      for (int i = 0; i < m; ++i) sb[i] = mkc(0, 0);
+    __syncwarp(gmask);
+    slab_stencil<P>(1, DS, sb, m, s, phn, gmask);
+    __syncwarp(gmask);
+    {
+      cxd* const bufs[1] = {buf};
+      group_solve_d0<P, 1>(thn, a.d0tab, G, bufs, s, gmask);
+    }
+    __syncwarp(gmask);
+    for (int r = s; r < ny; r += P) v1[r + 2] = buf[G.at(r)];
+  } else {
+    for (int r = s; r < ny; r += P) buf[G.at(r)] = a.R1[cb + r];
+    __syncwarp(gmask);
+    group_solve<P>(K_ETA, sc.lambda, a.ps.ni, kk, thn, DS, G, buf, fac, s, gmask);
+    __syncwarp(gmask);
+    const double rkk = c00 ? 0.0 : 1.0 / kk;
+    for (int r = s; r < ny; r += P) {
+      const cxd eta = buf[G.at(r)], dv = v1[r + 2];
+      cxd u, w;
+      if (c00) {
+        u = mkc(eta.x, 0.0);
+        w = mkc(eta.y, 0.0);
+      } else {
+        u = mkc((-al * dv.y + be * eta.y) * rkk, (al * dv.x - be * eta.x) * rkk);
+        w = mkc((-be * dv.y - al * eta.y) * rkk, (be * dv.x + al * eta.x) * rkk);
+      }
+      v1[r + 2] = u;
+      buf[G.at(r)] = w;
+    }
+    // __syncwarp orders the lanes' global stores before the ghost-row reads
+    __syncwarp(gmask);
+    for (int k = s; k < 4; k += P) {
+      const int srow = k == 0 ? 0 : (k == 1 ? 1 : (k == 2 ? ny - 1 : ny - 2));
+      const int drow = k == 0 ? ny : (k == 1 ? ny + 1 : (k == 2 ? -1 : -2));
+      v1[drow + 2] = cmul(v1[srow + 2], k < 2 ? phn : cconj(phn));
+    }
+    store_with_ghosts<P>(a.V3 + (size_t)cg * g.rows, buf, G, ny, phn, s, false);
+  }
+}
+
+// lines of shared memory a group holds in the persistent kernels (PART 0:
+// the solves, 1: the exact_shift shift alone, which takes its four lines
+// one at a time through one, 2, 3: the two halves of the solves)
+constexpr int solve_lines(int part) { return part == 0 ? 2 : 1; }
+
+// The solve stage (PART 0; 1: the exact_shift shift alone; 2, 3: the halves
+// of the solves) on a persistent grid: each group of P lanes walks the
+// columns col, col + gridDim.x groups, ...; shared memory holds only the
+// group's lines (solve_lines), and the group's factor scratch is its own
+// slice of a.facg in global memory, rewritten column after column (so it
+// stays in L2).  Fewer bytes of shared memory a warp let more warps share an
+// SM.
+template <int P, bool EXACT, int PART>
 #ifndef COLSOLVE_MINB
 #define COLSOLVE_MINB 8  // 128 registers: up to 16 single-warp blocks an SM
 #endif
@@ -546,14 +590,17 @@ __global__ void __launch_bounds__(64, COLSOLVE_MINB) k_column_solve(ColumnArgs a
   const int grp = threadIdx.x / P, s = threadIdx.x - grp * P;
   const int lineN = P * g.MS;
   const size_t facn = (size_t)(g.m - 2) * 4 * P;
-  const size_t per_group = (size_t)2 * lineN * 2 + (a.facg ? 0 : facn);  // doubles
+  const size_t per_group = (size_t)solve_lines(PART) * lineN * 2 + (a.facg ? 0 : facn);  // doubles
   cxd* bufA = reinterpret_cast<cxd*>(smem_d + per_group * grp);
   cxd* bufB = bufA + lineN;
   const int slot = blockIdx.x * groups + grp;
   // the factor scratch: the group's slice of a.facg, or after its lines
-  double* fac = a.facg ? a.facg + (size_t)slot * facn : reinterpret_cast<double*>(bufB + lineN);
+  double* fac = a.facg ? a.facg + (size_t)slot * facn : reinterpret_cast<double*>(bufA + solve_lines(PART) * lineN);
   for (int col = slot; col < g.ncol * g.nmem; col += gridDim.x * groups)
-    column_solve_body<P, EXACT, SHIFT_ONLY>(a, col, s, bufA, bufB, fac);
+    if constexpr (PART <= 1)
+      column_solve_body<P, EXACT, PART == 1>(a, col, s, bufA, bufB, fac);
+    else
+      column_solve_half<P, PART - 2>(a, col, s, bufA, fac);
 }
 
 // --------------------------------------------------------- k_line_solve ----
@@ -781,7 +828,8 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
   }
   // the untiled and fused forms read FP64 product spectra only (the
   // linear right-hand sides read none)
-  if (MODE != COL_SOLVE && MODE != COL_SHIFT && g.mp && NONLIN) return cudaErrorInvalidValue;
+  if (MODE != COL_SOLVE && MODE != COL_SHIFT && MODE != COL_SOLVE_V && MODE != COL_SOLVE_ETA && g.mp && NONLIN)
+    return cudaErrorInvalidValue;
   if (MODE == COL_RHS) {  // one warp per column, four per block, no shared memory
     const int blocks = (g.ncol * g.nmem + 3) / 4;
     k_column<32, EXACT, NONLIN, COL_RHS><<<blocks, 128, 0, st>>>(a);
@@ -792,8 +840,13 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
   // when the context has one (HST_COLUMN_GFAC), else in shared memory
   // the persistent solve stage when the context keeps the factor scratch in
   // global memory, else the one-column-per-group kernel
-  const bool gfac = (MODE == COL_SOLVE || (MODE == COL_SHIFT && EXACT)) && a.facg != nullptr;
-  const size_t per = gfac ? column_lines_bytes(g) + (a.facg ? 0 : column_fac_doubles(g) * sizeof(double))
+  constexpr int PART = MODE == COL_SHIFT ? 1 : (MODE == COL_SOLVE_V ? 2 : (MODE == COL_SOLVE_ETA ? 3 : 0));
+  const bool gfac =
+      (MODE == COL_SOLVE || (MODE == COL_SHIFT && EXACT) || MODE == COL_SOLVE_V || MODE == COL_SOLVE_ETA) &&
+      a.facg != nullptr;
+  if ((MODE == COL_SOLVE_V || MODE == COL_SOLVE_ETA) && (!gfac || EXACT)) return cudaErrorInvalidValue;
+  const size_t per = gfac ? column_lines_bytes(g) / 2 * solve_lines(PART) +
+                               (a.facg ? 0 : column_fac_doubles(g) * sizeof(double))
                           : column_smem_bytes(g, EXACT && MODE == COL_FUSED);
   int groups = (P >= 32 ? 32 : 64) / P;
   if (groups < 1) groups = 1;
@@ -803,7 +856,7 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
   size_t smem = per * groups;
   int blocks = (g.ncol * g.nmem + groups - 1) / groups;
   if (gfac) {
-    auto kern = k_column_solve<P, EXACT, MODE == COL_SHIFT>;
+    auto kern = k_column_solve<P, EXACT, PART>;
     smem_limit(*a.dstate, kern, 200 * 1024);
     // persistent: the blocks that are resident at once (at most 16 warps an
     // SM), and no more groups than the scratch has slices for
@@ -816,10 +869,14 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
     kern<<<blocks, T, smem, st>>>(a);
     return cudaGetLastError();
   }
-  auto kern = k_column<P, EXACT, NONLIN, MODE>;
-  smem_limit(*a.dstate, kern, 200 * 1024);
-  kern<<<blocks, T, smem, st>>>(a);
-  return cudaGetLastError();
+  if constexpr (MODE == COL_SOLVE_V || MODE == COL_SOLVE_ETA) {
+    return cudaErrorInvalidValue;
+  } else {
+    auto kern = k_column<P, EXACT, NONLIN, MODE>;
+    smem_limit(*a.dstate, kern, 200 * 1024);
+    kern<<<blocks, T, smem, st>>>(a);
+    return cudaGetLastError();
+  }
 }
 
 template <int P, bool EXACT, bool NONLIN>
@@ -828,6 +885,12 @@ static cudaError_t launch_column_m(const ColumnArgs& a, int part, cudaStream_t s
   if (part == COL_SOLVE) return launch_column_t<P, EXACT, NONLIN, COL_SOLVE>(a, st);
   if (part == COL_SHIFT) {
     if constexpr (EXACT && !NONLIN) return launch_column_t<P, true, false, COL_SHIFT>(a, st);
+    return cudaErrorInvalidValue;
+  }
+  if (part == COL_SOLVE_V || part == COL_SOLVE_ETA) {
+    if constexpr (!EXACT)
+      return part == COL_SOLVE_V ? launch_column_t<P, false, NONLIN, COL_SOLVE_V>(a, st)
+                                 : launch_column_t<P, false, NONLIN, COL_SOLVE_ETA>(a, st);
     return cudaErrorInvalidValue;
   }
   return launch_column_t<P, EXACT, NONLIN, COL_FUSED>(a, st);

@@ -90,10 +90,7 @@ __device__ __forceinline__ void zinv_body(const Geometry& g, const double2* __re
   fft_sel<NT, +1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
 }
 template <int NT, int PPT, typename C>
-#ifndef ZT768
-#define ZT768 0
-#endif
-__global__ void __launch_bounds__(PPT <= 8 ? (ZT768 ? 768 : 512) : 256) k_zinv(Geometry g, const double2* __restrict__ V0,
+__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256) k_zinv(Geometry g, const double2* __restrict__ V0,
                                               const double2* __restrict__ V1, const double2* __restrict__ V2,
                                               C* __restrict__ Z, const C* __restrict__ twz) {
   zinv_body<NT, PPT, C>(g, V0, V1, V2, Z, twz);
@@ -127,8 +124,8 @@ struct ZfwdDst {
 // 256; the same on k_zinv measured slower; the 8-point plans are held to
 // two blocks an SM)
 template <int NT, int PPT, typename C>
-__global__ void __launch_bounds__(PPT <= 8 ? (ZT768 ? 768 : 384) : 256, PPT <= 8 && !ZT768 ? 2 : 1) k_zfwd(Geometry g, const C* __restrict__ Pp, C* __restrict__ Q,
-                                              const C* __restrict__ twz) {
+__global__ void __launch_bounds__(PPT <= 8 ? 384 : 256, PPT <= 8 ? 2 : 1)
+    k_zfwd(Geometry g, const C* __restrict__ Pp, C* __restrict__ Q, const C* __restrict__ twz) {
   extern __shared__ double2 sh_d[];
   C* sh = reinterpret_cast<C*>(sh_d);
   const int yt = blockIdx.x, ix = blockIdx.y, p = blockIdx.z % 6, mem = blockIdx.z / 6;

@@ -106,6 +106,38 @@ def test_768x768x512_against_oracle():
     print(check_both("c3"))
 
 
+def test_768x768x512_mixed_statistics_3000_substeps():
+    """The mixed-precision form against the FP64 form over 3000 substeps of
+    the 768^2 x 512 workload from the same seeded field: the time averages of
+    the energy and the dissipation (hst_gpu_outstats, src/hst_stats.f90:136-285
+    on the device, every 30 substeps) agree within 0.5 %.  About three
+    minutes of device time."""
+    if device_bytes_free() < 40e9:
+        pytest.skip("the 768^2 x 512 context needs about 30 GB of device memory")
+    w = WORKLOADS["c3"]
+    deck = dict(w["deck"])
+    y = oracle.Sim(oracle.params_from_deck(dict(deck, nx=1, nz=1))).y()
+    V0 = seeded_field("c3", y)
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        s = hst.Solver(dict(deck, precision=prec))
+        s.time = 0.0
+        s.set_velocity(V0)
+        e, d = [], []
+        for _ in range(100):
+            s.timesteps(10, deck["deltat"])
+            st = s.outstats()
+            e.append(st["energy"])
+            d.append(st["diss"])
+        assert all(math.isfinite(v) for v in e + d)
+        runs[prec] = (float(np.mean(e)), float(np.mean(d)))
+        s.close()
+    (e64, d64), (emp, dmp) = runs["fp64"], runs["mixed"]
+    print("energy", e64, emp, "dissipation", d64, dmp)
+    assert abs(emp - e64) <= 5e-3 * abs(e64)
+    assert abs(dmp - d64) <= 5e-3 * abs(d64)
+
+
 @pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
 @pytest.mark.parametrize("axis", ["x", "z"])
 def test_768_plans_parity(prec, tol, axis):
