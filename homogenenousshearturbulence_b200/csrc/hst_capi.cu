@@ -381,7 +381,9 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
   // transform y tile (at most 512 threads for the 8-point z plans)
   g.Ty = 2;
   for (int t : {8, 4}) {
-    if (p.ny % t == 0 && (size_t)t * (g.nzd + 1) * 16 <= 100 * 1024 && (g.pptz != 8 || t * g.nzd / 8 <= 384)) {
+    // (the 8-point plans keep their lines padded, one element in eight)
+    const size_t line = g.pptz == 8 ? g.nzd + g.nzd / 8 + 8 : g.nzd + 1;
+    if (p.ny % t == 0 && (size_t)t * line * 16 <= 100 * 1024 && (g.pptz != 8 || t * g.nzd / 8 <= 384)) {
       g.Ty = t;
       break;
     }

@@ -183,6 +183,20 @@ struct ShLinesPT {
 };
 typedef ShLinesPT<cxd> ShLinesP;
 __host__ __device__ constexpr int ls_padded(int N) { return N + N / 8 + 1; }
+// The line stride of the same padded layout under the line-fastest mapping
+// of the z kernels (butterfly b: line b % nl, index b / nl, so that the
+// global loads and stores of nl adjacent rows coalesce): a wavefront's
+// lanes cover nl lines times S/nl consecutive indices (S = 128 / sizeof(C)
+// elements a bank row), and a stride of S/nl (mod S) with the pad in eight
+// spreads them over distinct banks in every stage of the 8-point plans
+// (nl in {2, 4, 8}).
+template <typename C>
+__host__ __device__ inline int ls_lines(int N, int nl) {
+  const int S = 128 / (int)sizeof(C);
+  const int target = (S / nl) % S;
+  const int base = N + N / 8;
+  return base + ((target - base) % S + S) % S;
+}
 
 // One radix-R stage.  Butterfly b of the block: line l = b % nl, index
 // j = b / nl.  Inputs ld(l, j + r N/R), outputs st(l, (j/Ns) Ns R + j%Ns + r Ns).
@@ -305,12 +319,20 @@ template <> struct Plan8<192> { static constexpr int n = 3, r0 = 8, r1 = 4, r2 =
 template <> struct Plan8<384> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 = 6; };
 template <> struct Plan8<768> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 = 12; };
 
-template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF, typename LD, typename ST, typename C>
-__device__ __forceinline__ void fft_fixed(int nl, const C* __restrict__ tw, C* sh, const LD& src, const ST& dst) {
+// PZ: the padded lines at stride ls_lines under the line-fastest mapping.
+// PP (three-stage plans): the second stage writes a second set of nl lines
+// at sh2 and the third reads them, so that neither stage reads and writes
+// the same lines (two barriers fewer); src must not overlap the lines at sh
+// and dst not those at sh2.
+template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF, bool PZ, bool PP, typename LD, typename ST,
+          typename C>
+__device__ __forceinline__ void fft_fixed(int nl, const C* __restrict__ tw, C* sh, const LD& src, const ST& dst,
+                                          C* sh2) {
   using PL = std::conditional_t<(PPT <= 8), Plan8<N>, Plan<N>>;
   static_assert(PL::n > 0, "no compile-time plan for this length and points per thread");
-  using LT = std::conditional_t<JF, ShLinesPT<C>, ShLinesT<C>>;
-  const LT L = {sh, JF ? ls_padded(N) : N + 1};
+  static_assert(!(JF && PZ), "PZ is the line-fastest mapping's layout");
+  using LT = std::conditional_t<JF || PZ, ShLinesPT<C>, ShLinesT<C>>;
+  const LT L = {sh, JF ? ls_padded(N) : (PZ ? ls_lines<C>(N, nl) : N + 1)};
   if constexpr (PL::n == 1) {
     fft_stage_io<PL::r0, S, PPT, SRC_SH && DST_SH, LD, ST, JF, C>(N, nl, 1, tw, src, dst);
   } else if constexpr (PL::n == 2) {
@@ -322,18 +344,27 @@ __device__ __forceinline__ void fft_fixed(int nl, const C* __restrict__ tw, C* s
     const C* tw3 = JF ? tw + (PL::r1 - 1) * PL::r0 : tw;
     fft_stage_io<PL::r0, S, PPT, SRC_SH, LD, LT, JF, C>(N, nl, 1, tw, src, L);
     __syncthreads();
-    fft_stage_io<PL::r1, S, PPT, true, LT, LT, JF, C>(N, nl, PL::r0, tw, L, L);
-    __syncthreads();
-    fft_stage_io<PL::r2, S, PPT, DST_SH, LT, ST, JF, C>(N, nl, PL::r0 * PL::r1, tw3, L, dst);
+    if constexpr (PP) {
+      const LT L2 = {sh2, L.LS};
+      fft_stage_io<PL::r1, S, PPT, false, LT, LT, JF, C>(N, nl, PL::r0, tw, L, L2);
+      __syncthreads();
+      fft_stage_io<PL::r2, S, PPT, false, LT, ST, JF, C>(N, nl, PL::r0 * PL::r1, tw3, L2, dst);
+    } else {
+      fft_stage_io<PL::r1, S, PPT, true, LT, LT, JF, C>(N, nl, PL::r0, tw, L, L);
+      __syncthreads();
+      fft_stage_io<PL::r2, S, PPT, DST_SH, LT, ST, JF, C>(N, nl, PL::r0 * PL::r1, tw3, L, dst);
+    }
   }
 }
 
 // NT > 0: the compile-time plan of length NT; NT = 0: the runtime plan of N.
-template <int NT, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF = false, typename LD, typename ST, typename C>
+template <int NT, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF = false, bool PZ = false, bool PP = false,
+          typename LD, typename ST, typename C>
 __device__ __forceinline__ void fft_sel(int N, int nl, const C* __restrict__ tw, C* sh, const LD& src,
-                                        const ST& dst) {
+                                        const ST& dst, C* sh2 = nullptr) {
+  static_assert(!(PZ || PP) || NT > 0, "PZ and PP need a compile-time plan");
   if constexpr (NT > 0) {
-    fft_fixed<NT, S, PPT, SRC_SH, DST_SH, JF>(nl, tw, sh, src, dst);
+    fft_fixed<NT, S, PPT, SRC_SH, DST_SH, JF, PZ, PP>(nl, tw, sh, src, dst, sh2);
   } else {
     fft_global<S, PPT, SRC_SH, DST_SH>(N, nl, tw, sh, src, dst);
   }

@@ -346,6 +346,7 @@ __device__ __forceinline__ void slab_stencil(int n, const SlabDer& DS, cxd* sb, 
   }
 }
 
+
 // The solve stage on one column, for MODE COL_SOLVE (and COL_SHIFT: the
 // exact_shift shift alone) with the lines and every intermediate in shared
 // memory: no scratch column of V is written and read back.
@@ -543,18 +544,27 @@ __device__ __forceinline__ void column_solve_half(const ColumnArgs& a, int cg, i
     group_solve<P>(K_ETA, sc.lambda, a.ps.ni, kk, thn, DS, G, buf, fac, s, gmask);
     __syncwarp(gmask);
     const double rkk = c00 ? 0.0 : 1.0 / kk;
-    for (int r = s; r < ny; r += P) {
-      const cxd eta = buf[G.at(r)], dv = v1[r + 2];
-      cxd u, w;
-      if (c00) {
-        u = mkc(eta.x, 0.0);
-        w = mkc(eta.y, 0.0);
-      } else {
-        u = mkc((-al * dv.y + be * eta.y) * rkk, (al * dv.x - be * eta.x) * rkk);
-        w = mkc((-be * dv.y - al * eta.y) * rkk, (be * dv.x + al * eta.x) * rkk);
+    // dv/dy eight rows at a time, every load issued before the first use
+    for (int r0 = s; r0 < ny; r0 += 8 * P) {
+      cxd dvb[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) dvb[k] = r0 + k * P < ny ? v1[r0 + k * P + 2] : mkc(0, 0);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int r = r0 + k * P;
+        if (r >= ny) break;
+        const cxd eta = buf[G.at(r)], dv = dvb[k];
+        cxd u, w;
+        if (c00) {
+          u = mkc(eta.x, 0.0);
+          w = mkc(eta.y, 0.0);
+        } else {
+          u = mkc((-al * dv.y + be * eta.y) * rkk, (al * dv.x - be * eta.x) * rkk);
+          w = mkc((-be * dv.y - al * eta.y) * rkk, (be * dv.x + al * eta.x) * rkk);
+        }
+        v1[r + 2] = u;
+        buf[G.at(r)] = w;
       }
-      v1[r + 2] = u;
-      buf[G.at(r)] = w;
     }
     // __syncwarp orders the lanes' global stores before the ghost-row reads
     __syncwarp(gmask);
@@ -590,12 +600,14 @@ __global__ void __launch_bounds__(64, COLSOLVE_MINB) k_column_solve(ColumnArgs a
   const int grp = threadIdx.x / P, s = threadIdx.x - grp * P;
   const int lineN = P * g.MS;
   const size_t facn = (size_t)(g.m - 2) * 4 * P;
-  const size_t per_group = (size_t)solve_lines(PART) * lineN * 2 + (a.facg ? 0 : facn);  // doubles
+  const size_t per_group = (size_t)solve_lines(PART) * lineN * 2;  // doubles
   cxd* bufA = reinterpret_cast<cxd*>(smem_d + per_group * grp);
   cxd* bufB = bufA + lineN;
   const int slot = blockIdx.x * groups + grp;
-  // the factor scratch: the group's slice of a.facg, or after its lines
-  double* fac = a.facg ? a.facg + (size_t)slot * facn : reinterpret_cast<double*>(bufA + solve_lines(PART) * lineN);
+  // the factor scratch: the group's slice of a.facg (the launcher runs this
+  // kernel only when the context has one)
+  if (a.facg == nullptr) return;
+  double* fac = a.facg + (size_t)slot * facn;
   for (int col = slot; col < g.ncol * g.nmem; col += gridDim.x * groups)
     if constexpr (PART <= 1)
       column_solve_body<P, EXACT, PART == 1>(a, col, s, bufA, bufB, fac);
@@ -840,11 +852,10 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
   // when the context has one (HST_COLUMN_GFAC), else in shared memory
   // the persistent solve stage when the context keeps the factor scratch in
   // global memory, else the one-column-per-group kernel
-  constexpr int PART = MODE == COL_SHIFT ? 1 : (MODE == COL_SOLVE_V ? 2 : (MODE == COL_SOLVE_ETA ? 3 : 0));
-  const bool gfac =
-      (MODE == COL_SOLVE || (MODE == COL_SHIFT && EXACT) || MODE == COL_SOLVE_V || MODE == COL_SOLVE_ETA) &&
-      a.facg != nullptr;
-  if ((MODE == COL_SOLVE_V || MODE == COL_SOLVE_ETA) && (!gfac || EXACT)) return cudaErrorInvalidValue;
+  constexpr bool HALVES = MODE == COL_SOLVE_V || MODE == COL_SOLVE_ETA;
+  constexpr int PART = MODE == COL_SHIFT ? 1 : MODE == COL_SOLVE_V ? 2 : MODE == COL_SOLVE_ETA ? 3 : 0;
+  const bool gfac = (MODE == COL_SOLVE || (MODE == COL_SHIFT && EXACT) || HALVES) && a.facg != nullptr;
+  if (HALVES && (!gfac || EXACT)) return cudaErrorInvalidValue;
   const size_t per = gfac ? column_lines_bytes(g) / 2 * solve_lines(PART) +
                                (a.facg ? 0 : column_fac_doubles(g) * sizeof(double))
                           : column_smem_bytes(g, EXACT && MODE == COL_FUSED);
@@ -869,7 +880,7 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
     kern<<<blocks, T, smem, st>>>(a);
     return cudaGetLastError();
   }
-  if constexpr (MODE == COL_SOLVE_V || MODE == COL_SOLVE_ETA) {
+  if constexpr (HALVES) {
     return cudaErrorInvalidValue;
   } else {
     auto kern = k_column<P, EXACT, NONLIN, MODE>;

@@ -74,6 +74,14 @@ struct TileSrc {
   __device__ __forceinline__ C operator()(int yi, int kz) const { return base[(size_t)kz * zstride + yi]; }
 };
 
+// the z kernels' 8-point plans keep their lines padded (ls_lines), free of
+// bank conflicts under the line-fastest mapping
+__host__ __device__ constexpr bool z_padded(int NT, int PPT) { return NT > 0 && PPT <= 8; }
+template <int NT, int PPT, typename C>
+__host__ __device__ inline size_t z_smem(int nzd, int Ty) {
+  return (size_t)Ty * (z_padded(NT, PPT) ? ls_lines<C>(nzd, Ty) : nzd + 1) * sizeof(C);
+}
+
 template <int NT, int PPT, typename C>
 __device__ __forceinline__ void zinv_body(const Geometry& g, const double2* __restrict__ V0,
                                           const double2* __restrict__ V1, const double2* __restrict__ V2,
@@ -87,12 +95,12 @@ __device__ __forceinline__ void zinv_body(const Geometry& g, const double2* __re
   const ZinvSrc<C> src = {V + (size_t)ix * g.nzT * g.rows + (g.edge_gap ? 0 : 2) + yt * Ty, g.rows, g.nz, NZ,
                           g.edge_gap};
   const TileDst<C> dst = {Z + (((size_t)c * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
-  fft_sel<NT, +1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
+  fft_sel<NT, +1, PPT, false, false, false, z_padded(NT, PPT)>(NZ, Ty, twz, sh, src, dst);
 }
 template <int NT, int PPT, typename C>
-__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256) k_zinv(Geometry g, const double2* __restrict__ V0,
-                                              const double2* __restrict__ V1, const double2* __restrict__ V2,
-                                              C* __restrict__ Z, const C* __restrict__ twz) {
+__global__ void __launch_bounds__(PPT <= 8 ? 512 : 256)
+    k_zinv(Geometry g, const double2* __restrict__ V0, const double2* __restrict__ V1, const double2* __restrict__ V2,
+           C* __restrict__ Z, const C* __restrict__ twz) {
   zinv_body<NT, PPT, C>(g, V0, V1, V2, Z, twz);
 }
 // the FP32 1536-point plan (192 threads) held to three blocks an SM (an
@@ -122,9 +130,11 @@ struct ZfwdDst {
 // (the explicit one-block minimum lets the compiler take 160 registers
 // for the 16-point plans, which measured 0.46 against 0.50 ms at 384^2 x
 // 256; the same on k_zinv measured slower; the 8-point plans are held to
-// two blocks an SM)
+// three blocks an SM: at 768^2 x 512 4.68 against 5.19 ms for two in FP64,
+// where the kernel waits on its global loads, while the z-inverse measured
+// slower held to two or three)
 template <int NT, int PPT, typename C>
-__global__ void __launch_bounds__(PPT <= 8 ? 384 : 256, PPT <= 8 ? 2 : 1)
+__global__ void __launch_bounds__(PPT <= 8 ? 384 : 256, PPT <= 8 ? 3 : 1)
     k_zfwd(Geometry g, const C* __restrict__ Pp, C* __restrict__ Q, const C* __restrict__ twz) {
   extern __shared__ double2 sh_d[];
   C* sh = reinterpret_cast<C*>(sh_d);
@@ -134,7 +144,7 @@ __global__ void __launch_bounds__(PPT <= 8 ? 384 : 256, PPT <= 8 ? 2 : 1)
   Q += (size_t)mem * 6 * g.ncol * g.ny;
   const TileSrc<C> src = {Pp + (((size_t)p * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
   const ZfwdDst<C> dst = {Q + ((size_t)p * g.ncol + (size_t)ix * g.nzT) * g.ny + yt * Ty, g.ny, g.nz, NZ};
-  fft_sel<NT, -1, PPT, false, false>(NZ, Ty, twz, sh, src, dst);
+  fft_sel<NT, -1, PPT, false, false, false, z_padded(NT, PPT)>(NZ, Ty, twz, sh, src, dst);
 }
 
 // -------------------------------------------------------------- k_xprod ----
@@ -213,6 +223,9 @@ struct ProdSrc {
 
 #ifndef XPROD_MINB
 #define XPROD_MINB 3
+#endif
+#ifndef XPROD_PP
+#define XPROD_PP 0
 #endif
 // launch bounds of k_xprod: 6 NX / PPT threads; the 8-point plan at 384
 // is held to 72 registers so that three 288-thread blocks fit an SM, the
@@ -300,8 +313,11 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
     }
     __syncthreads();
     if (!tile_ok) return;
+    // the three inverse lines ping-pong between lines 0..2 and 3..5 (the
+    // tile in lies in 3..5 at 768 points, read by the first stage only)
     const XinvSh<C> xs = {stg, nxB, nx, NX};
-    fft_sel<NT, +1, PPT, false, true, JF>(NX, 3, twx + NX, sh, xs, L);
+    constexpr bool PP = XPROD_PP && Plan8<NT>::n == 3;
+    fft_sel<NT, +1, PPT, false, true, JF, false, PP>(NX, 3, twx + NX, sh, xs, L, sh + 3 * LS);
   } else {
     const XinvSrc<C> xs = {Z + tile + yi0, cs, Ty, nx, NX};
     fft_sel<NT, +1, PPT, false, true, JF>(NX, 3, twx, sh, xs, L);
@@ -636,10 +652,10 @@ static cudaError_t launch_zinv_main(const Geometry& g, const DeviceState& d, cud
   const dim3 grid(g.ny / g.Ty, g.nxB, 3 * g.nmem);
   if (g.mp) {
     typedef float2 C;
-    const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
     C* Z = reinterpret_cast<C*>(d.Z);
 #define HST_ZINV(NT, PPT)                                                                                     \
   {                                                                                                           \
+    const size_t smem = z_smem<NT, PPT, C>(g.nzd, g.Ty);                                                      \
     if (NT == 1536) {                                                                                         \
       big_smem(d, k_zinv_1536f);                                                                                 \
       k_zinv_1536f<<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], Z, d.twzf);          \
@@ -653,9 +669,9 @@ static cudaError_t launch_zinv_main(const Geometry& g, const DeviceState& d, cud
     return cudaGetLastError();
   }
   typedef double2 C;
-  const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
 #define HST_ZINV(NT, PPT)                                                                                     \
   {                                                                                                           \
+    const size_t smem = z_smem<NT, PPT, C>(g.nzd, g.Ty);                                                      \
     big_smem(d, k_zinv<NT, PPT, C>);                                                                             \
     k_zinv<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], d.Z, d.twz);     \
   }
@@ -669,11 +685,11 @@ static cudaError_t launch_zfwd_main(const Geometry& g, const DeviceState& d, cud
   const dim3 grid(g.ny / g.Ty, g.nxB, 6 * g.nmem);
   if (g.mp) {
     typedef float2 C;
-    const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
     const C* Pp = reinterpret_cast<const C*>(d.Pp);
     C* Q = reinterpret_cast<C*>(d.Q);
 #define HST_ZFWD(NT, PPT)                                                                  \
   {                                                                                        \
+    const size_t smem = z_smem<NT, PPT, C>(g.nzd, g.Ty);                                   \
     big_smem(d, k_zfwd<NT, PPT, C>);                                                          \
     k_zfwd<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, Pp, Q, d.twzf);       \
   }
@@ -682,9 +698,9 @@ static cudaError_t launch_zfwd_main(const Geometry& g, const DeviceState& d, cud
     return cudaGetLastError();
   }
   typedef double2 C;
-  const size_t smem = (size_t)g.Ty * (g.nzd + 1) * sizeof(C);
 #define HST_ZFWD(NT, PPT)                                                                  \
   {                                                                                        \
+    const size_t smem = z_smem<NT, PPT, C>(g.nzd, g.Ty);                                   \
     big_smem(d, k_zfwd<NT, PPT, C>);                                                          \
     k_zfwd<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.Pp, d.Q, d.twz);    \
   }

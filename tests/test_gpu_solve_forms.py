@@ -22,28 +22,34 @@ CASES = {
 }
 
 
-def solver_with(deck, halves, V0):
-    old = os.environ.get("HST_SOLVE_HALVES")
-    os.environ["HST_SOLVE_HALVES"] = "1" if halves else "0"
+FORMS = {"one_pass": dict(HST_SOLVE_HALVES="0"), "halves": dict(HST_SOLVE_HALVES="1")}
+
+
+def solver_with(deck, form, V0):
+    env = FORMS[form]
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
     try:
         s, o = make_pair(deck, V0)
     finally:
-        if old is None:
-            del os.environ["HST_SOLVE_HALVES"]
-        else:
-            os.environ["HST_SOLVE_HALVES"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
     return s, o
 
 
+@pytest.mark.parametrize("form", ["halves"])
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_solve_halves_same_bits(case):
+def test_solve_forms_same_bits(case, form):
     """3 time steps of a 512-row deck with the solves in one pass and in two
     halves: identical velocity bits and CFL number; the halves within the
     precision's bound of the oracle."""
     deck = c1_deck(**CASES[case])
     V0 = seeded_field(deck, seed=6, k0=4.0, energy=0.1)
-    s1, _ = solver_with(deck, False, V0)
-    s2, o = solver_with(deck, True, V0)
+    s1, _ = solver_with(deck, "one_pass", V0)
+    s2, o = solver_with(deck, form, V0)
     for _ in range(3):
         s1.timestep(deck["deltat"])
     V2, Vo = run_pair(s2, o, deck["deltat"], 3)
