@@ -135,17 +135,25 @@ __device__ __forceinline__ double derv(const double* __restrict__ der, int ny, i
 // m rows per lane: derS[((n*5 + j)*m + i)*P + s] = der(s*m + i, n, j - 2),
 // so that the P lanes reading row i of their own slabs read consecutive
 // addresses.
-struct SlabDer {
+// SH: the table (or its first slices) copied into shared memory
+template <bool SH = false>
+struct SlabDerT {
   const double* __restrict__ p;
   int m, P;
   __device__ __forceinline__ double operator()(int s, int i, int n, int j) const {
-    return __ldg(p + ((size_t)((n * 5 + j) * m + i)) * P + s);
+    const double* q = p + ((size_t)((n * 5 + j) * m + i)) * P + s;
+    if constexpr (SH)
+      return *q;
+    else
+      return __ldg(q);
   }
 };
+typedef SlabDerT<false> SlabDer;
 
 // The five band entries of row i of slab s of system `sys` before the wrap
 // phase: coef, src/hst_linsolve.f90:236-252.
-__device__ __forceinline__ void row_coefs(int sys, double lambda, double ni, double kk, const SlabDer& D, int s, int i,
+template <class DST>
+__device__ __forceinline__ void row_coefs(int sys, double lambda, double ni, double kk, const DST& D, int s, int i,
                                           double a[5]) {
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
@@ -286,8 +294,8 @@ struct LineGeom {
 // buf: the line (right-hand side in, solution out), in LineGeom layout.
 // fac: per-lane factor scratch, (m-2) x 4 x P doubles.
 // Rows of the right-hand side of KIND_DY must already hold D1 src.
-template <int P>
-__device__ void group_solve(int sys, double lambda, double ni, double kk, double theta, const SlabDer& DS,
+template <int P, class DST = SlabDer>
+__device__ void group_solve(int sys, double lambda, double ni, double kk, double theta, const DST& DS,
                             const LineGeom& G, cxd* buf, double* fac, int s, unsigned gmask) {
   const int m = G.m, mi = m - 2, MS = G.MS;
   cxd* sb = buf + s * MS;
@@ -603,11 +611,16 @@ __device__ void d0_factor(const SlabDer& DS, int m, int s, unsigned gmask, doubl
 // group_solve for the D0 matrix from the table of d0_factor, on NR lines
 // at once (buf[k] each as group_solve's buf): the lines share every table
 // load and run as independent dependency chains
-template <int P, int NR>
+template <int P, int NR, bool SH = false>
 __device__ void group_solve_d0(double theta, const double* __restrict__ tab, const LineGeom& G, cxd* const* buf,
                                int s, unsigned gmask) {
   const int m = G.m, mi = m - 2, MS = G.MS;
-  auto T = [&](int f) { return __ldg(tab + (size_t)f * P + s); };
+  auto T = [&](int f) {
+    if constexpr (SH)
+      return tab[(size_t)f * P + s];
+    else
+      return __ldg(tab + (size_t)f * P + s);
+  };
   auto T2 = [&](int f) { return M2{T(f), T(f + 1), T(f + 2), T(f + 3)}; };
   cxd* sb[NR];
   cxd x1[NR], x2[NR], sx0[NR], sx1[NR];

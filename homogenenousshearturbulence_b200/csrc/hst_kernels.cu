@@ -310,8 +310,8 @@ __device__ __forceinline__ void column_body(const ColumnArgs& a, int cg, int s, 
 // across the box edge, the shear-periodic ghost images f(ny + k) = f(k) ph,
 // f(-k) = f(ny - k) conj(ph) (wrap_rows, src/hst_mpi.f90:340-355).  The sum
 // runs over j = -2..2 in order, as the reference's stencils do.
-template <int P>
-__device__ __forceinline__ void slab_stencil(int n, const SlabDer& DS, cxd* sb, int m, int s, cxd ph, unsigned gmask) {
+template <int P, class DST>
+__device__ __forceinline__ void slab_stencil(int n, const DST& DS, cxd* sb, int m, int s, cxd ph, unsigned gmask) {
   const cxd f0 = sb[0], f1 = sb[1], l0 = sb[m - 2], l1 = sb[m - 1];
   const int up = (s + 1) & (P - 1), dn = (s - 1) & (P - 1);
   cxd a0 = shfl_c(gmask, f0, up, P), a1 = shfl_c(gmask, f1, up, P);  // rows s m + m, s m + m + 1
@@ -357,9 +357,13 @@ __device__ __forceinline__ void slab_stencil(int n, const SlabDer& DS, cxd* sb, 
 //   then linsolve (:298-326): D2V and ETA solves, v with its ghost rows to
 //   V2, D1 stencil of v and the DY solve (table) in place, u and w, V1 and
 //   V3 with their ghost rows.
-template <int P, bool EXACT, bool SHIFT_ONLY>
+// SHT (the shift alone): the D0 table and the D0 slice of der are read from
+// the block's shared copies d0s and der0s instead of global memory
+template <int P, bool EXACT, bool SHIFT_ONLY, bool SHT = false>
 __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, int s, cxd* bufA, cxd* bufB,
-                                                  double* fac) {
+                                                  double* fac, const double* d0s = nullptr,
+                                                  const double* der0s = nullptr) {
+  static_assert(!SHT || SHIFT_ONLY, "shared tables for the shift alone");
   const Geometry& g = a.g;
   const int mem = cg / g.ncol, col = cg - mem * g.ncol;
   const int ny = g.ny, nz = g.nz, nzT = g.nzT, m = g.m;
@@ -400,7 +404,7 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, i
       __syncwarp(gmask);
       {
         cxd* const bufs[1] = {X};
-        group_solve_d0<P, 1>(th0, a.d0tab, G, bufs, s, gmask);
+        group_solve_d0<P, 1, SHT>(th0, SHT ? d0s : a.d0tab, G, bufs, s, gmask);
       }
       __syncwarp(gmask);
       cxd e = e0;
@@ -410,7 +414,10 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, i
         e = cmul(e, estep);
       }
       __syncwarp(gmask);
-      slab_stencil<P>(0, DS, sX, m, s, phs, gmask);
+      if constexpr (SHT)
+        slab_stencil<P>(0, SlabDerT<true>{der0s, m, P}, sX, m, s, phs, gmask);
+      else
+        slab_stencil<P>(0, DS, sX, m, s, phs, gmask);
       __syncwarp(gmask);
       if (q < 2 || SHIFT_ONLY) {
         double2* dst = q == 0 ? a.O1 : (q == 1 ? a.O2 : (q == 2 ? a.R1 : a.R2));
@@ -498,8 +505,11 @@ __global__ void k_column(ColumnArgs a) {
 // writes u over it (then u's ghost rows) and w (V3 with its ghost rows).
 // The same operations in the same order as the one-pass form, so the same
 // bits.
-template <int P, int HALF>
-__device__ __forceinline__ void column_solve_half(const ColumnArgs& a, int cg, int s, cxd* buf, double* fac) {
+// SHT: der (its first nsl slices, D0 D1 D2 D4 in that order) read from the
+// block's shared copy ders
+template <int P, int HALF, bool SHT = false>
+__device__ __forceinline__ void column_solve_half(const ColumnArgs& a, int cg, int s, cxd* buf, double* fac,
+                                                  const double* ders = nullptr) {
   const Geometry& g = a.g;
   const int mem = cg / g.ncol, col = cg - mem * g.ncol;
   const int ny = g.ny, nz = g.nz, nzT = g.nzT, m = g.m;
@@ -516,7 +526,7 @@ __device__ __forceinline__ void column_solve_half(const ColumnArgs& a, int cg, i
   const double kk = al * al + be * be;
   const SubstepScalars& sc = a.sc;
   const size_t cb = (size_t)cg * g.rows + 2;  // row 0 of the column
-  const SlabDer DS = {a.derS, m, P};
+  const SlabDerT<SHT> DS = {SHT ? ders : a.derS, m, P};
   cxd* const sb = buf + s * G.MS;
   const double thn = al * sc.sx_n + be * sc.sz_n;
   const cxd phn = cexpi(-thn);
@@ -613,6 +623,58 @@ __global__ void __launch_bounds__(64, COLSOLVE_MINB) k_column_solve(ColumnArgs a
       column_solve_body<P, EXACT, PART == 1>(a, col, s, bufA, bufB, fac);
     else
       column_solve_half<P, PART - 2>(a, col, s, bufA, fac);
+}
+
+// The exact_shift shift alone with the D0 table and the D0 slice of der in
+// shared memory, shared by the block's warps (one group of P = 32 lanes a
+// warp, one line each): a persistent grid of one block an SM.
+#ifndef HST_SHIFT_SHT
+#define HST_SHIFT_SHT 1
+#endif
+#ifndef HST_HALF_SHT
+#define HST_HALF_SHT 1
+#endif
+__host__ __device__ inline size_t shift_sht_tables(int m, int P) {
+  return ((size_t)d0_fields(m, P) * P + (size_t)5 * m * P) * sizeof(double);
+}
+template <int P>
+__global__ void __launch_bounds__(512, 1) k_column_shift_sht(ColumnArgs a) {
+  extern __shared__ double smem_d[];
+  const Geometry& g = a.g;
+  const int groups = blockDim.x / P;
+  const int grp = threadIdx.x / P, s = threadIdx.x - grp * P;
+  const int ntab = d0_fields(g.m, P) * P, nder = 5 * g.m * P;
+  double* const d0s = smem_d;
+  double* const der0s = d0s + ntab;
+  for (int i = threadIdx.x; i < ntab; i += blockDim.x) d0s[i] = a.d0tab[i];
+  for (int i = threadIdx.x; i < nder; i += blockDim.x) der0s[i] = a.derS[i];
+  __syncthreads();
+  cxd* const bufA = reinterpret_cast<cxd*>(der0s + nder) + (size_t)grp * P * g.MS;
+  for (int col = blockIdx.x * groups + grp; col < g.ncol * g.nmem; col += gridDim.x * groups)
+    column_solve_body<P, true, true, true>(a, col, s, bufA, bufA, nullptr, d0s, der0s);
+}
+
+// The halves of the solves with der in shared memory (HALF 0 reads all four
+// slices, HALF 1 the D0 and D2 slices, copied as the first three), shared
+// by the block's warps, one group of P = 32 lanes and one line a warp: a
+// persistent grid of one block an SM.
+__host__ __device__ inline int half_der_slices(int half) { return half == 0 ? 4 : 3; }
+template <int P, int HALF>
+__global__ void __launch_bounds__(512, 1) k_column_half_sht(ColumnArgs a) {
+  extern __shared__ double smem_d[];
+  const Geometry& g = a.g;
+  const int groups = blockDim.x / P;
+  const int grp = threadIdx.x / P, s = threadIdx.x - grp * P;
+  const int nder = half_der_slices(HALF) * 5 * g.m * P;
+  double* const ders = smem_d;
+  for (int i = threadIdx.x; i < nder; i += blockDim.x) ders[i] = a.derS[i];
+  __syncthreads();
+  if (a.facg == nullptr) return;
+  cxd* const buf = reinterpret_cast<cxd*>(ders + nder) + (size_t)grp * P * g.MS;
+  const int slot = blockIdx.x * groups + grp;
+  double* const fac = a.facg + (size_t)slot * (g.m - 2) * 4 * P;
+  for (int col = slot; col < g.ncol * g.nmem; col += gridDim.x * groups)
+    column_solve_half<P, HALF, true>(a, col, s, buf, fac, ders);
 }
 
 // --------------------------------------------------------- k_line_solve ----
@@ -866,6 +928,40 @@ static cudaError_t launch_column_t(const ColumnArgs& a, cudaStream_t st) {
   const int T = groups * P;
   size_t smem = per * groups;
   int blocks = (g.ncol * g.nmem + groups - 1) / groups;
+  if constexpr (MODE == COL_SHIFT && EXACT && P == 32) {
+    if (HST_SHIFT_SHT) {
+      // warps a block: as many lines as fit beside the tables, at most 16
+      const size_t tabs = shift_sht_tables(g.m, P), line = column_lines_bytes(g) / 2;
+      const int W = (int)std::min<size_t>(16, (227 * 1024 - tabs) / line);
+      if (W >= 4) {
+        const size_t sm = tabs + (size_t)W * line;
+        smem_limit(*a.dstate, k_column_shift_sht<P>, 227 * 1024);
+        const int nsm = a.dstate->nsm > 0 ? a.dstate->nsm : 148;
+        const int nb = std::min(nsm, (g.ncol * g.nmem + W - 1) / W);
+        k_column_shift_sht<P><<<nb, 32 * W, sm, st>>>(a);
+        return cudaGetLastError();
+      }
+    }
+  }
+  if constexpr ((MODE == COL_SOLVE_V || MODE == COL_SOLVE_ETA) && P == 32) {
+    // the halves with der in shared memory (the factor scratch in global
+    // memory): warps a block, as many lines as fit beside der, at most 16
+    if (HST_HALF_SHT && gfac) {
+      const int half = MODE == COL_SOLVE_V ? 0 : 1;
+      const size_t tabs = (size_t)half_der_slices(half) * 5 * g.m * P * sizeof(double);
+      const size_t line = column_lines_bytes(g) / 2;
+      const int W = (int)std::min<size_t>(16, tabs < 227 * 1024 ? (227 * 1024 - tabs) / line : 0);
+      const int nsm = a.dstate->nsm > 0 ? a.dstate->nsm : 148;
+      if (W >= 4 && nsm * W <= a.fac_groups) {
+        auto kh = half == 0 ? k_column_half_sht<P, 0> : k_column_half_sht<P, 1>;
+        const size_t sm = tabs + (size_t)W * line;
+        smem_limit(*a.dstate, kh, 227 * 1024);
+        const int nb = std::min(nsm, (g.ncol * g.nmem + W - 1) / W);
+        kh<<<nb, 32 * W, sm, st>>>(a);
+        return cudaGetLastError();
+      }
+    }
+  }
   if (gfac) {
     auto kern = k_column_solve<P, EXACT, PART>;
     smem_limit(*a.dstate, kern, 200 * 1024);
