@@ -420,6 +420,33 @@ static std::vector<double> slab_major(const std::vector<double>& der, int ny, in
   return o;
 }
 
+// der's distinct rows (equal bits) coefficient-major, and each row's index
+// among them, for hst::DerRows; nu = 0 when there are more than DER_ROWS_MAX
+constexpr int DER_ROWS_MAX = 256;
+static int der_rows(const std::vector<double>& der, int ny, std::vector<double>& tab, std::vector<int>& idx) {
+  std::unordered_map<std::string, int> seen;
+  std::vector<int> first;
+  idx.assign(ny, 0);
+  for (int r = 0; r < ny; ++r) {
+    std::string key(20 * sizeof(double), '\0');
+    for (int q = 0; q < 20; ++q) std::memcpy(&key[q * sizeof(double)], &der[(size_t)r + (size_t)ny * q], sizeof(double));
+    auto it = seen.find(key);
+    if (it == seen.end()) {
+      it = seen.emplace(std::move(key), (int)first.size()).first;
+      first.push_back(r);
+    }
+    idx[r] = it->second;
+  }
+  const int nu = (int)first.size();
+  if (nu > DER_ROWS_MAX) return 0;
+  tab.assign((size_t)20 * nu, 0.0);
+  for (int q = 0; q < 20; ++q)
+    for (int u = 0; u < nu; ++u) tab[(size_t)q * nu + u] = der[(size_t)first[u] + (size_t)ny * q];
+  return nu;
+}
+// uploads der's distinct-row table (stream-ordered after everything before)
+static cudaError_t upload_der_rows(hst_ctx* ctx);
+
 static std::vector<double2> twiddles(int n) {
   std::vector<double2> t(n);
   for (int k = 0; k < n; ++k) {
@@ -445,7 +472,7 @@ static void free_device(hst_ctx* c) {
   for (int i = 0; i < 7; ++i)
     if (d.F[i]) cudaFree(d.F[i]);
   void* ps[] = {d.Z,    d.Pp,   d.Q,    d.der,  d.derS,  d.d0tab, d.y,    d.dyl,  d.gdamp, d.twx, d.twz,
-                d.twxf, d.twzf, d.cfl,  d.stats, d.vvdz, d.vvdx,  d.vvdp, d.Zg,   d.Ppg,  d.Qg};
+                d.twxf, d.twzf, d.cfl,  d.stats, d.vvdz, d.vvdx,  d.vvdp, d.Zg,   d.Ppg,  d.Qg,  d.derU, d.derI};
   for (void* q : ps)
     if (q) cudaFree(q);
   if (d.facg) cudaFree(d.facg);
@@ -594,6 +621,8 @@ static int create_context(const hst_gpu_params* pin, int nmem, hst_ctx** out) {
   }
   ok = ok && alloc((void**)&d.der, sizeof(double) * 20 * (size_t)ny);
   ok = ok && alloc((void**)&d.derS, sizeof(double) * 20 * (size_t)ny);
+  ok = ok && alloc((void**)&d.derU, sizeof(double) * 20 * (size_t)DER_ROWS_MAX);
+  ok = ok && alloc((void**)&d.derI, sizeof(int) * (size_t)ny);
   ok = ok && alloc((void**)&d.d0tab, sizeof(double) * hst::d0_table_doubles(ny));
   ok = ok && alloc((void**)&d.y, sizeof(double) * (ny + 4));
   ok = ok && alloc((void**)&d.dyl, sizeof(double) * ny);
@@ -629,6 +658,7 @@ static int create_context(const hst_gpu_params* pin, int nmem, hst_ctx** out) {
     auto ds = slab_major(ctx->der, ny, g.P, g.m);
     cudaMemcpy(d.derS, ds.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice);
     etab = hst::launch_d0_table(g, d, ctx->stream);
+    if (etab == cudaSuccess) etab = upload_der_rows(ctx);
   }
   cudaMemcpy(d.y, ctx->y.data(), sizeof(double) * (ny + 4), cudaMemcpyHostToDevice);
   cudaMemcpy(d.dyl, ctx->dyl.data(), sizeof(double) * ny, cudaMemcpyHostToDevice);
@@ -748,6 +778,22 @@ extern "C" int hst_gpu_destroy(hst_ctx* ctx) {
   return HST_OK;
 }
 
+static cudaError_t upload_der_rows(hst_ctx* ctx) {
+  std::vector<double> tab;
+  std::vector<int> idx;
+  const int ny = ctx->p.ny;
+  const int nu = der_rows(ctx->der, ny, tab, idx);
+  // the kernels queued before may still read the previous table
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess && nu > 0) e = cudaMemcpy(ctx->d.derU, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(ctx->d.derI, idx.data(), sizeof(int) * ny, cudaMemcpyHostToDevice);
+  ctx->d.nderU = e == cudaSuccess ? nu : 0;
+  ctx->db.derU = ctx->d.derU;
+  ctx->db.derI = ctx->d.derI;
+  ctx->db.nderU = ctx->d.nderU;
+  return e;
+}
+
 extern "C" const char* hst_gpu_last_error(const hst_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
 extern "C" long long hst_gpu_launch_count(const hst_ctx* ctx) { return ctx ? ctx->launches : 0; }
 extern "C" void* hst_gpu_stream(const hst_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
@@ -762,6 +808,7 @@ extern "C" int hst_gpu_set_tables(hst_ctx* ctx, const double* der, const double*
     auto ds = slab_major(ctx->der, ny, ctx->g.P, ctx->g.m);
     CK(cudaMemcpy(ctx->d.derS, ds.data(), sizeof(double) * 20 * ny, cudaMemcpyHostToDevice));
     CK(hst::launch_d0_table(ctx->g, ctx->d, ctx->stream));
+    CK(upload_der_rows(ctx));
   }
   if (y) {
     std::memcpy(ctx->y.data(), y, sizeof(double) * (ny + 4));

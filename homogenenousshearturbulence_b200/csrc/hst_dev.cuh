@@ -130,6 +130,25 @@ enum { K_D2V = 1, K_ETA = 2, K_POISSON = 3, K_D0 = 4, K_DY = 5 };
 __device__ __forceinline__ double derv(const double* __restrict__ der, int ny, int iy, int n, int j) {
   return __ldg(der + iy + ny * (n + 4 * (j + 2)));
 }
+// der(iy, n, j) through a table of its distinct rows: row iy of der is row
+// idx[iy] of tab, stored coefficient-major (tab[(n + 4 (j + 2)) nu + u]) so
+// that the lanes of a warp, whose rows map to a few distinct rows, read a
+// few neighbouring words.  On a uniform grid ny rows have a few dozen
+// distinct coefficient sets (rounding of the grid differences), so the
+// table stays in L1 where der itself (20 ny doubles) does not.
+struct DerRows {
+  const double* __restrict__ tab;
+  const int* __restrict__ idx;
+  int nu;
+  __device__ __forceinline__ double operator()(int iy, int n, int j) const {
+    return __ldg(tab + (n + 4 * (j + 2)) * nu + __ldg(idx + iy));
+  }
+};
+struct DerFull {
+  const double* __restrict__ der;
+  int ny;
+  __device__ __forceinline__ double operator()(int iy, int n, int j) const { return derv(der, ny, iy, n, j); }
+};
 
 // The same table in slab-major order for a line-solve group of P lanes and
 // m rows per lane: derS[((n*5 + j)*m + i)*P + s] = der(s*m + i, n, j - 2),

@@ -41,6 +41,9 @@ struct DeviceState {
   double2* Q;           // spectral products: [6][ncol][ny]
   double* der;          // der(0:ny-1, 0:3, -2:2)
   double* derS;         // the same, slab-major for the line-solve groups (SlabDer)
+  double* derU;         // der's distinct rows, coefficient-major (DerRows); nderU of them, 0: not used
+  int* derI;            // the distinct row of each row
+  int nderU;
   double* d0tab;        // the D0 matrix factored for the line-solve group (d0_factor)
   double* y;            // y(-2:ny+1)
   double* dyl;          // dyl(0:ny-1)

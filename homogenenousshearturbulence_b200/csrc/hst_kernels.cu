@@ -36,6 +36,9 @@ struct ColumnArgs {
   const double2* Qg;  // the ghost rows' product spectra [6][ncol][4] (null: their wrap images)
   const double* der;
   const double* derS;
+  const double* derU;  // the distinct rows of der (DerRows), or null
+  const int* derI;
+  int nderU;
   const double* d0tab;
   const double* y;
   const double* gdamp;
@@ -134,7 +137,7 @@ __device__ __forceinline__ void column_body(const ColumnArgs& a, int cg, int s, 
       cxd r1, r2, o1, o2;
       const double yr = a.y[r + 2];
       auto fsh = [&]() { return cexpi(-(cc.al * sc.dgx + cc.be * sc.dgz) * yr); };
-      rhs_point<NONLIN, EXACT>(cc, sc, der, ny, r, fsh, tv, tq, a.O1[ro], a.O2[ro], r1, r2, o1, o2);
+      rhs_point<NONLIN, EXACT>(cc, sc, DerFull{der, ny}, ny, r, fsh, tv, tq, a.O1[ro], a.O2[ro], r1, r2, o1, o2);
       a.O1[ro] = o1;
       a.O2[ro] = o2;
       if (MODE == COL_RHS) {
@@ -628,6 +631,9 @@ __global__ void __launch_bounds__(64, COLSOLVE_MINB) k_column_solve(ColumnArgs a
 // The exact_shift shift alone with the D0 table and the D0 slice of der in
 // shared memory, shared by the block's warps (one group of P = 32 lanes a
 // warp, one line each): a persistent grid of one block an SM.
+#ifndef HST_DER_ROWS
+#define HST_DER_ROWS 1  // the right-hand sides read der through its table of distinct rows
+#endif
 #ifndef HST_SHIFT_SHT
 #define HST_SHIFT_SHT 1
 #endif
@@ -859,8 +865,12 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
       if (REC && sc.yuni) return fbase;
       return cexpi(-(cc.al * sc.dgx + cc.be * sc.dgz) * yr);
     };
-    rhs_point<NONLIN, EXACT>(cc, sc, a.der, ny, r, fsh, tv, tq, S[9 * RT_W + lane], S[9 * RT_W + 32 + lane], r1,
-                             r2, o1, o2);
+    if (a.derU)
+      rhs_point<NONLIN, EXACT>(cc, sc, DerRows{a.derU, a.derI, a.nderU}, ny, r, fsh, tv, tq, S[9 * RT_W + lane],
+                               S[9 * RT_W + 32 + lane], r1, r2, o1, o2);
+    else
+      rhs_point<NONLIN, EXACT>(cc, sc, DerFull{a.der, ny}, ny, r, fsh, tv, tq, S[9 * RT_W + lane],
+                               S[9 * RT_W + 32 + lane], r1, r2, o1, o2);
     if (REC) fbase = cmul(fbase, fstep);
     const size_t ro = cbase + 2 + r;
     a.O1[ro] = o1;
@@ -1027,6 +1037,9 @@ cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysSca
   a.Qg = d.Qg;
   a.der = d.der;
   a.derS = d.derS;
+  a.derU = HST_DER_ROWS && d.nderU > 0 ? d.derU : nullptr;
+  a.derI = d.derI;
+  a.nderU = d.nderU;
   a.d0tab = d.d0tab;
   a.y = d.y;
   a.gdamp = d.gdamp;

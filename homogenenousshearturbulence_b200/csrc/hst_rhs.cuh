@@ -97,19 +97,19 @@ __device__ __forceinline__ void product_rhs(int p, const ColConst& c, double ode
 #ifndef HST_MIXED_RHS_FP32
 #define HST_MIXED_RHS_FP32 1  // 0: the mixed form's right-hand sides in FP64 but for the product stencils
 #endif
-template <bool NONLIN, bool EXACT, class TV, class TQ, class FS>
-__device__ __forceinline__ void rhs_point(const ColConst& c, const SubstepScalars& sc, const double* __restrict__ der,
-                                          int ny, int r, const FS& fsh, const TV& tv, const TQ& tq, cxd o1in, cxd o2in,
-                                          cxd& r1, cxd& r2, cxd& o1, cxd& o2) {
+template <bool NONLIN, bool EXACT, class TV, class TQ, class FS, class DA>
+__device__ __forceinline__ void rhs_point(const ColConst& c, const SubstepScalars& sc, const DA& der, int ny, int r,
+                                          const FS& fsh, const TV& tv, const TQ& tq, cxd o1in, cxd o2in, cxd& r1,
+                                          cxd& r2, cxd& o1, cxd& o2) {
   const double kk = c.kk, al = c.al, be = c.be, ni = c.ni, gs = c.gs;
   constexpr bool F32 = sizeof(decltype(tq(0, 0))) == 8;
   double d0[5], d1[5], d2[5], d4[5];
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
-    d0[j] = derv(der, ny, r, 0, j - 2);
-    d1[j] = derv(der, ny, r, 1, j - 2);
-    d2[j] = derv(der, ny, r, 2, j - 2);
-    d4[j] = derv(der, ny, r, 3, j - 2);
+    d0[j] = der(r, 0, j - 2);
+    d1[j] = der(r, 1, j - 2);
+    d2[j] = der(r, 2, j - 2);
+    d4[j] = der(r, 3, j - 2);
   }
   if constexpr (!F32 || !HST_MIXED_RHS_FP32) {
     // v equation
