@@ -421,8 +421,7 @@ static std::vector<double> slab_major(const std::vector<double>& der, int ny, in
 }
 
 // der's distinct rows (equal bits) coefficient-major, and each row's index
-// among them, for hst::DerRows; nu = 0 when there are more than DER_ROWS_MAX
-constexpr int DER_ROWS_MAX = 256;
+// among them, for hst::DerRows (nu <= ny: a stretched grid keeps them all)
 static int der_rows(const std::vector<double>& der, int ny, std::vector<double>& tab, std::vector<int>& idx) {
   std::unordered_map<std::string, int> seen;
   std::vector<int> first;
@@ -438,7 +437,6 @@ static int der_rows(const std::vector<double>& der, int ny, std::vector<double>&
     idx[r] = it->second;
   }
   const int nu = (int)first.size();
-  if (nu > DER_ROWS_MAX) return 0;
   tab.assign((size_t)20 * nu, 0.0);
   for (int q = 0; q < 20; ++q)
     for (int u = 0; u < nu; ++u) tab[(size_t)q * nu + u] = der[(size_t)first[u] + (size_t)ny * q];
@@ -621,7 +619,7 @@ static int create_context(const hst_gpu_params* pin, int nmem, hst_ctx** out) {
   }
   ok = ok && alloc((void**)&d.der, sizeof(double) * 20 * (size_t)ny);
   ok = ok && alloc((void**)&d.derS, sizeof(double) * 20 * (size_t)ny);
-  ok = ok && alloc((void**)&d.derU, sizeof(double) * 20 * (size_t)DER_ROWS_MAX);
+  ok = ok && alloc((void**)&d.derU, sizeof(double) * 20 * (size_t)ny);
   ok = ok && alloc((void**)&d.derI, sizeof(int) * (size_t)ny);
   ok = ok && alloc((void**)&d.d0tab, sizeof(double) * hst::d0_table_doubles(ny));
   ok = ok && alloc((void**)&d.y, sizeof(double) * (ny + 4));

@@ -631,9 +631,6 @@ __global__ void __launch_bounds__(64, COLSOLVE_MINB) k_column_solve(ColumnArgs a
 // The exact_shift shift alone with the D0 table and the D0 slice of der in
 // shared memory, shared by the block's warps (one group of P = 32 lanes a
 // warp, one line each): a persistent grid of one block an SM.
-#ifndef HST_DER_ROWS
-#define HST_DER_ROWS 1  // the right-hand sides read der through its table of distinct rows
-#endif
 #ifndef HST_SHIFT_SHT
 #define HST_SHIFT_SHT 1
 #endif
@@ -865,12 +862,8 @@ __global__ void __launch_bounds__(32 * RT_WARPS, RT_MINB) k_rhs_tiled(ColumnArgs
       if (REC && sc.yuni) return fbase;
       return cexpi(-(cc.al * sc.dgx + cc.be * sc.dgz) * yr);
     };
-    if (a.derU)
-      rhs_point<NONLIN, EXACT>(cc, sc, DerRows{a.derU, a.derI, a.nderU}, ny, r, fsh, tv, tq, S[9 * RT_W + lane],
-                               S[9 * RT_W + 32 + lane], r1, r2, o1, o2);
-    else
-      rhs_point<NONLIN, EXACT>(cc, sc, DerFull{a.der, ny}, ny, r, fsh, tv, tq, S[9 * RT_W + lane],
-                               S[9 * RT_W + 32 + lane], r1, r2, o1, o2);
+    rhs_point<NONLIN, EXACT>(cc, sc, DerRows{a.derU, a.derI, a.nderU}, ny, r, fsh, tv, tq, S[9 * RT_W + lane],
+                             S[9 * RT_W + 32 + lane], r1, r2, o1, o2);
     if (REC) fbase = cmul(fbase, fstep);
     const size_t ro = cbase + 2 + r;
     a.O1[ro] = o1;
@@ -1037,7 +1030,7 @@ cudaError_t launch_column(const Geometry& g, const DeviceState& d, const PhysSca
   a.Qg = d.Qg;
   a.der = d.der;
   a.derS = d.derS;
-  a.derU = HST_DER_ROWS && d.nderU > 0 ? d.derU : nullptr;
+  a.derU = d.derU;
   a.derI = d.derI;
   a.nderU = d.nderU;
   a.d0tab = d.d0tab;
