@@ -381,9 +381,10 @@ static int choose_geometry(const hst_gpu_params& p, Geometry& g, std::string& wh
   // transform y tile (at most 512 threads for the 8-point z plans)
   g.Ty = 2;
   for (int t : {8, 4}) {
-    // (the 8-point plans keep their lines padded, one element in eight)
-    const size_t line = g.pptz == 8 ? g.nzd + g.nzd / 8 + 8 : g.nzd + 1;
-    if (p.ny % t == 0 && (size_t)t * line * 16 <= 100 * 1024 && (g.pptz != 8 || t * g.nzd / 8 <= 384)) {
+    // (the lines are padded, one element in eight for the 8-point plans, in
+    // sixteen for the others: two blocks of up to 112 KB share an SM)
+    const size_t line = g.pptz == 8 ? g.nzd + g.nzd / 8 + 8 : g.nzd + g.nzd / 16 + 8;
+    if (p.ny % t == 0 && (size_t)t * line * 16 <= 112 * 1024 && (g.pptz != 8 || t * g.nzd / 8 <= 384)) {
       g.Ty = t;
       break;
     }

@@ -174,12 +174,14 @@ typedef ShLinesT<cxd> ShLines;
 // The same with one pad element after every 8: with butterflies mapped
 // index-fastest (JF) the radix-8/6/12 exchanges of the 8-point plans are
 // then free of bank conflicts.  Line stride ls_padded(N).
-template <typename C>
+// (SH: one pad element in 2^SH; 3 for the 8-point plans, 4 for the
+// 16-point plans of the z kernels, whose first radix is 16)
+template <typename C, int SH = 3>
 struct ShLinesPT {
   C* p;
   int LS;
-  __device__ __forceinline__ C operator()(int l, int i) const { return p[l * LS + i + (i >> 3)]; }
-  __device__ __forceinline__ void operator()(int l, int i, C v) const { p[l * LS + i + (i >> 3)] = v; }
+  __device__ __forceinline__ C operator()(int l, int i) const { return p[l * LS + i + (i >> SH)]; }
+  __device__ __forceinline__ void operator()(int l, int i, C v) const { p[l * LS + i + (i >> SH)] = v; }
 };
 typedef ShLinesPT<cxd> ShLinesP;
 __host__ __device__ constexpr int ls_padded(int N) { return N + N / 8 + 1; }
@@ -190,11 +192,11 @@ __host__ __device__ constexpr int ls_padded(int N) { return N + N / 8 + 1; }
 // elements a bank row), and a stride of S/nl (mod S) with the pad in eight
 // spreads them over distinct banks in every stage of the 8-point plans
 // (nl in {2, 4, 8}).
-template <typename C>
+template <typename C, int SH = 3>
 __host__ __device__ inline int ls_lines(int N, int nl) {
   const int S = 128 / (int)sizeof(C);
   const int target = (S / nl) % S;
-  const int base = N + N / 8;
+  const int base = N + (N >> SH);
   return base + ((target - base) % S + S) % S;
 }
 
@@ -324,15 +326,18 @@ template <> struct Plan8<768> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 =
 // at sh2 and the third reads them, so that neither stage reads and writes
 // the same lines (two barriers fewer); src must not overlap the lines at sh
 // and dst not those at sh2.
-template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF, bool PZ, bool PP, typename LD, typename ST,
-          typename C>
+// XSH > 0: the caller's padded layout, one pad in 2^XSH at line stride lsx.
+template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF, bool PZ, bool PP, int XSH, typename LD,
+          typename ST, typename C>
 __device__ __forceinline__ void fft_fixed(int nl, const C* __restrict__ tw, C* sh, const LD& src, const ST& dst,
-                                          C* sh2) {
+                                          C* sh2, int lsx) {
   using PL = std::conditional_t<(PPT <= 8), Plan8<N>, Plan<N>>;
   static_assert(PL::n > 0, "no compile-time plan for this length and points per thread");
-  static_assert(!(JF && PZ), "PZ is the line-fastest mapping's layout");
-  using LT = std::conditional_t<JF || PZ, ShLinesPT<C>, ShLinesT<C>>;
-  const LT L = {sh, JF ? ls_padded(N) : (PZ ? ls_lines<C>(N, nl) : N + 1)};
+  static_assert(!(JF && (PZ || XSH > 0)), "PZ and XSH are the line-fastest mapping's layouts");
+  // the pad follows the plan's first radix (8 or 16), or the caller's
+  constexpr int PSH = XSH > 0 ? XSH : (PPT <= 8 ? 3 : 4);
+  using LT = std::conditional_t<JF, ShLinesPT<C>, std::conditional_t<(PZ || XSH > 0), ShLinesPT<C, PSH>, ShLinesT<C>>>;
+  const LT L = {sh, JF ? ls_padded(N) : (XSH > 0 ? lsx : (PZ ? ls_lines<C, PSH>(N, nl) : N + 1))};
   if constexpr (PL::n == 1) {
     fft_stage_io<PL::r0, S, PPT, SRC_SH && DST_SH, LD, ST, JF, C>(N, nl, 1, tw, src, dst);
   } else if constexpr (PL::n == 2) {
@@ -359,12 +364,12 @@ __device__ __forceinline__ void fft_fixed(int nl, const C* __restrict__ tw, C* s
 
 // NT > 0: the compile-time plan of length NT; NT = 0: the runtime plan of N.
 template <int NT, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF = false, bool PZ = false, bool PP = false,
-          typename LD, typename ST, typename C>
+          int XSH = 0, typename LD, typename ST, typename C>
 __device__ __forceinline__ void fft_sel(int N, int nl, const C* __restrict__ tw, C* sh, const LD& src,
-                                        const ST& dst, C* sh2 = nullptr) {
-  static_assert(!(PZ || PP) || NT > 0, "PZ and PP need a compile-time plan");
+                                        const ST& dst, C* sh2 = nullptr, int lsx = 0) {
+  static_assert(!(PZ || PP || XSH > 0) || NT > 0, "PZ, PP and XSH need a compile-time plan");
   if constexpr (NT > 0) {
-    fft_fixed<NT, S, PPT, SRC_SH, DST_SH, JF, PZ, PP>(nl, tw, sh, src, dst, sh2);
+    fft_fixed<NT, S, PPT, SRC_SH, DST_SH, JF, PZ, PP, XSH>(nl, tw, sh, src, dst, sh2, lsx);
   } else {
     fft_global<S, PPT, SRC_SH, DST_SH>(N, nl, tw, sh, src, dst);
   }

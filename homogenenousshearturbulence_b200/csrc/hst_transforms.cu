@@ -37,6 +37,9 @@ cudaError_t set_fft_constants() {
 
 bool fft_length_ok(int n) { return plan_ok(n); }
 
+#ifndef ZPAD16
+#define ZPAD16 1  // 0: the 16- and 32-point z plans on unpadded lines
+#endif
 // The order of the z kernels' blocks: IXF = 1 runs the x modes of one y tile
 // side by side (consecutive blocks read, or write, adjacent 64-byte runs of
 // the [yt][kz][ix][Ty] tiles of Z and Pp), 0 the y tiles of one x mode.
@@ -87,12 +90,22 @@ struct TileSrc {
   __device__ __forceinline__ C operator()(int yi, int kz) const { return base[(size_t)kz * zstride + yi]; }
 };
 
-// the z kernels' 8-point plans keep their lines padded (ls_lines), free of
-// bank conflicts under the line-fastest mapping
-__host__ __device__ constexpr bool z_padded(int NT, int PPT) { return NT > 0 && PPT <= 8; }
+// the z kernels' compile-time plans keep their lines padded (ls_lines: one
+// pad in 8 for the 8-point plans, in 16 for the 16- and 32-point plans),
+// free of bank conflicts under the line-fastest mapping
+// (FP64 16- and 32-point plans stay unpadded: at 384 points their eight
+// rows a block are conflict-free anyway, and at 1536 the pad measured
+// slower, 15.8 against 12.5 ms z-inverse and 27.0 against 23.6 ms
+// z-forward, where in FP32 it gains, 12.2 against 13.2 and 15.6 against
+// 17.8 ms)
+template <int NT, int PPT, typename C>
+__host__ __device__ constexpr bool z_padded() {
+  return NT > 0 && (PPT <= 8 || (ZPAD16 && sizeof(C) == 8));
+}
 template <int NT, int PPT, typename C>
 __host__ __device__ inline size_t z_smem(int nzd, int Ty) {
-  return (size_t)Ty * (z_padded(NT, PPT) ? ls_lines<C>(nzd, Ty) : nzd + 1) * sizeof(C);
+  const int ls = !z_padded<NT, PPT, C>() ? nzd + 1 : (PPT <= 8 ? ls_lines<C, 3>(nzd, Ty) : ls_lines<C, 4>(nzd, Ty));
+  return (size_t)Ty * ls * sizeof(C);
 }
 
 template <int NT, int PPT, typename C>
@@ -109,13 +122,22 @@ __device__ __forceinline__ void zinv_body(const Geometry& g, const double2* __re
   const ZinvSrc<C> src = {V + (size_t)ix * g.nzT * g.rows + (g.edge_gap ? 0 : 2) + yt * Ty, g.rows, g.nz, NZ,
                           g.edge_gap};
   const TileDst<C> dst = {Z + (((size_t)c * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
-  fft_sel<NT, +1, PPT, false, false, false, z_padded(NT, PPT)>(NZ, Ty, twz, sh, src, dst);
+  fft_sel<NT, +1, PPT, false, false, false, z_padded<NT, PPT, C>()>(NZ, Ty, twz, sh, src, dst);
 }
 template <int NT, int PPT, typename C>
 __global__ void __launch_bounds__(PPT <= 8 ? 512 : 256)
     k_zinv(Geometry g, const double2* __restrict__ V0, const double2* __restrict__ V1, const double2* __restrict__ V2,
            C* __restrict__ Z, const C* __restrict__ twz) {
   zinv_body<NT, PPT, C>(g, V0, V1, V2, Z, twz);
+}
+// the FP64 32-point plans (192 threads) held to two blocks an SM (1536
+// points: 16.5 -> 12.5 ms at 1536^2 x 512; an explicit block minimum on
+// the kernel above made the 384-point plan slower, 0.42 against 0.25 ms)
+template <int NT>
+__global__ void __launch_bounds__(192, 2) k_zinv_32(Geometry g, const double2* __restrict__ V0,
+                                                    const double2* __restrict__ V1, const double2* __restrict__ V2,
+                                                    double2* __restrict__ Z, const double2* __restrict__ twz) {
+  zinv_body<NT, 32, double2>(g, V0, V1, V2, Z, twz);
 }
 // the FP32 1536-point plan (192 threads) held to three blocks an SM (an
 // explicit block minimum on the kernel above made the 384-point plan slower)
@@ -148,7 +170,8 @@ struct ZfwdDst {
 // where the kernel waits on its global loads, while the z-inverse measured
 // slower held to two or three)
 template <int NT, int PPT, typename C>
-__global__ void __launch_bounds__(PPT <= 8 ? 384 : 256, PPT <= 8 ? 3 : 1)
+__global__ void __launch_bounds__(PPT <= 8 ? 384 : (PPT == 32 && NT > 0 ? 192 : 256),
+                                  PPT <= 8 ? 3 : (PPT == 32 && NT > 0 ? 2 : 1))
     k_zfwd(Geometry g, const C* __restrict__ Pp, C* __restrict__ Q, const C* __restrict__ twz) {
   extern __shared__ double2 sh_d[];
   C* sh = reinterpret_cast<C*>(sh_d);
@@ -159,7 +182,7 @@ __global__ void __launch_bounds__(PPT <= 8 ? 384 : 256, PPT <= 8 ? 3 : 1)
   Q += (size_t)mem * 6 * g.ncol * g.ny;
   const TileSrc<C> src = {Pp + (((size_t)p * nyT + yt) * NZ) * g.nxB * Ty + (size_t)ix * Ty, (size_t)g.nxB * Ty};
   const ZfwdDst<C> dst = {Q + ((size_t)p * g.ncol + (size_t)ix * g.nzT) * g.ny + yt * Ty, g.ny, g.nz, NZ};
-  fft_sel<NT, -1, PPT, false, false, false, z_padded(NT, PPT)>(NZ, Ty, twz, sh, src, dst);
+  fft_sel<NT, -1, PPT, false, false, false, z_padded<NT, PPT, C>()>(NZ, Ty, twz, sh, src, dst);
 }
 
 // -------------------------------------------------------------- k_xprod ----
@@ -242,6 +265,13 @@ struct ProdSrc {
 #ifndef XPROD_PP
 #define XPROD_PP 1
 #endif
+#ifndef XPAD1536
+#define XPAD1536 1
+#endif
+// line stride of the padded 1536-point x lines: 1728 + 3 (FP64) or + 11
+// (FP32), the strides that a CPU count of the plan's shared accesses ranks
+// best for three and six lines side by side
+__host__ __device__ constexpr int xls_1536(int elem) { return elem == 16 ? 1731 : 1739; }
 // launch bounds of k_xprod: 6 NX / PPT threads; the 8-point plan at 384
 // is held to 72 registers so that three 288-thread blocks fit an SM, the
 // FP32 32-point plan at 1536 to two blocks
@@ -287,8 +317,13 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   // 8-point plans: butterflies index-fastest over padded shared lines, the
   // tile in and out by TMA
   constexpr bool JF = (PPT <= 8 && NT > 0);
-  using LT = std::conditional_t<JF, ShLinesPT<C>, ShLinesT<C>>;
-  const int NX = 2 * g.nxd, nx = g.nx, nxB = g.nxB, NZ = g.nzd, Ty = g.Ty, LS = JF ? ls_padded(NX) : NX + 1;
+  // the 1536-point plan (butterflies line-fastest): lines padded one in
+  // eight at the stride xls_1536 (fewer bank conflicts for both the three
+  // inverse and the six forward lines)
+  constexpr int XSH = (!JF && NT == 1536 && XPAD1536) ? 3 : 0;
+  using LT = std::conditional_t<JF, ShLinesPT<C>, std::conditional_t<XSH != 0, ShLinesPT<C, 3>, ShLinesT<C>>>;
+  const int NX = 2 * g.nxd, nx = g.nx, nxB = g.nxB, NZ = g.nzd, Ty = g.Ty;
+  const int LS = JF ? ls_padded(NX) : (XSH ? xls_1536((int)sizeof(C)) : NX + 1);
   const int nyT = g.ny / Ty;
   const int y0 = 2 * blockIdx.x, kz = blockIdx.y % g.nzd, mem = blockIdx.y / g.nzd;
   Z += (size_t)mem * 3 * g.nzd * g.ny * g.nxB;
@@ -335,7 +370,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
     fft_sel<NT, +1, PPT, false, true, JF, false, PP>(NX, 3, twx + NX, sh, xs, L, sh + 3 * LS);
   } else {
     const XinvSrc<C> xs = {Z + tile + yi0, cs, Ty, nx, NX};
-    fft_sel<NT, +1, PPT, false, true, JF>(NX, 3, twx, sh, xs, L);
+    fft_sel<NT, +1, PPT, false, true, JF, false, false, XSH>(NX, 3, twx, sh, xs, L, sh, LS);
   }
   __syncthreads();
   if (want_cfl) {
@@ -355,7 +390,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   }
   // the six product lines, transformed forward in place
   const ProdSrc<LT, C> ps6 = {L, (T)ps.factor};
-  fft_sel<NT, -1, PPT, true, true, JF>(NX, 6, JF ? twx + NX : twx, sh, ps6, L);
+  fft_sel<NT, -1, PPT, true, true, JF, false, false, XSH>(NX, 6, JF ? twx + NX : twx, sh, ps6, L, sh, LS);
   __syncthreads();
   // separate the two real transforms of each line, keep kx = 0..nx
   if constexpr (ALIAS) {
@@ -687,8 +722,13 @@ static cudaError_t launch_zinv_main(const Geometry& g, const DeviceState& d, cud
 #define HST_ZINV(NT, PPT)                                                                                     \
   {                                                                                                           \
     const size_t smem = z_smem<NT, PPT, C>(g.nzd, g.Ty);                                                      \
-    big_smem(d, k_zinv<NT, PPT, C>);                                                                             \
-    k_zinv<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], d.Z, d.twz);     \
+    if (PPT == 32 && NT > 0) {                                                                                \
+      big_smem(d, k_zinv_32<NT>);                                                                             \
+      k_zinv_32<NT><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], d.Z, d.twz);        \
+    } else {                                                                                                  \
+      big_smem(d, k_zinv<NT, PPT, C>);                                                                        \
+      k_zinv<NT, PPT, C><<<grid, fft_threads(pts, PPT), smem, st>>>(g, d.F[0], d.F[1], d.F[2], d.Z, d.twz);   \
+    }                                                                                                         \
   }
   HST_FFT_DISPATCH(g.nzd, pts, g.pptz == 8, HST_ZINV);
 #undef HST_ZINV
@@ -732,7 +772,8 @@ static cudaError_t launch_xprod_main(const Geometry& g, const DeviceState& d, co
   const dim3 grid(g.ny / 2, g.nzd * g.nmem);
   if (g.mp) {
     typedef float2 C;
-    const size_t smem = !xprod_uses_maps(g) ? (size_t)6 * (NX + 1) * sizeof(C)
+    const size_t lines = (size_t)6 * (NX == 1536 && XPAD1536 ? xls_1536(8) : NX + 1) * sizeof(C);
+    const size_t smem = !xprod_uses_maps(g) ? lines
                         : (NX == 768 ? xprod_alias_smem(NX, sizeof(C)) : xprod_tma_smem(NX, g.nxB, sizeof(C)));
     const C* Z = reinterpret_cast<const C*>(d.Z);
     C* Pp = reinterpret_cast<C*>(d.Pp);
@@ -747,7 +788,8 @@ static cudaError_t launch_xprod_main(const Geometry& g, const DeviceState& d, co
     return cudaGetLastError();
   }
   typedef double2 C;
-  const size_t smem = !xprod_uses_maps(g) ? (size_t)6 * (NX + 1) * sizeof(C)
+  const size_t lines = (size_t)6 * (NX == 1536 && XPAD1536 ? xls_1536(16) : NX + 1) * sizeof(C);
+  const size_t smem = !xprod_uses_maps(g) ? lines
                       : (NX == 768 && g.pptx == 8 ? xprod_alias_smem(NX, sizeof(C))
                                                   : xprod_tma_smem(NX, g.nxB, sizeof(C)));
 #define HST_XPROD(NT, PPT)                                                                                    \
