@@ -268,6 +268,9 @@ struct ProdSrc {
 #ifndef XPAD1536
 #define XPAD1536 1
 #endif
+#ifndef XPROD_IL
+#define XPROD_IL 0
+#endif
 // line stride of the padded 1536-point x lines: 1728 + 3 (FP64) or + 11
 // (FP32), the strides that a CPU count of the plan's shared accesses ranks
 // best for three and six lines side by side
@@ -295,16 +298,25 @@ constexpr int XPROD_WAIT_LIMIT = 1 << 22;  // polls of the tile's TMA barrier be
 // the next 128-byte address (tensor copies need 128-byte aligned shared
 // addresses, and the dynamic shared base is only known to be 16-byte
 // aligned), then the mbarrier and the tile flag
-__host__ __device__ inline int xprod_stage_off(int NX) { return 6 * ls_padded(NX); }
+// the x kernel's padded line stride: at least ls_padded(NX), and 3 LS half
+// a bank row modulo a bank row (S = 128 / elem elements), for the
+// separation's alternating reads of lines pl and pl + 3
+__host__ __device__ constexpr int ls_x(int NX, int elem) {
+  const int S = 128 / elem, base = ls_padded(NX);
+  return elem == 16 ? base + (((S / 2 - base) % S) + S) % S : base;
+}
+__host__ __device__ inline int xprod_stage_off(int NX, int elem) { return 6 * ls_x(NX, elem); }
 __host__ __device__ inline size_t xprod_tma_smem(int NX, int nxB, size_t elem) {
-  return ((size_t)xprod_stage_off(NX) + 12 * (size_t)nxB + 2) * elem + 128;
+  return ((size_t)xprod_stage_off(NX, (int)elem) + 12 * (size_t)nxB + 2) * elem + 128;
 }
 // At 768 points the staging tiles live inside the six lines instead (the
 // tile in where lines 3..5 are, which the three inverse lines never touch;
 // the tile out over the lines once they have been read), so that a block
 // needs 6 padded lines of shared memory and two blocks share an SM
 __host__ __device__ constexpr bool xprod_alias(int NT, int PPT) { return PPT <= 8 && NT == 768; }
-__host__ __device__ inline size_t xprod_alias_smem(int NX, size_t elem) { return (size_t)6 * ls_padded(NX) * elem + 128; }
+__host__ __device__ inline size_t xprod_alias_smem(int NX, size_t elem) {
+  return (size_t)6 * ls_x(NX, (int)elem) * elem + 128;
+}
 
 template <int NT, int PPT, typename C>
 __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, PPT, (int)sizeof(C)))
@@ -323,7 +335,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   constexpr int XSH = (!JF && NT == 1536 && XPAD1536) ? 3 : 0;
   using LT = std::conditional_t<JF, ShLinesPT<C>, std::conditional_t<XSH != 0, ShLinesPT<C, 3>, ShLinesT<C>>>;
   const int NX = 2 * g.nxd, nx = g.nx, nxB = g.nxB, NZ = g.nzd, Ty = g.Ty;
-  const int LS = JF ? ls_padded(NX) : (XSH ? xls_1536((int)sizeof(C)) : NX + 1);
+  const int LS = JF ? ls_x(NX, (int)sizeof(C)) : (XSH ? xls_1536((int)sizeof(C)) : NX + 1);
   const int nyT = g.ny / Ty;
   const int y0 = 2 * blockIdx.x, kz = blockIdx.y % g.nzd, mem = blockIdx.y / g.nzd;
   Z += (size_t)mem * 3 * g.nzd * g.ny * g.nxB;
@@ -334,7 +346,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   const LT L = {sh, LS};
   constexpr bool ALIAS = xprod_alias(NT, PPT);
   auto align128 = [](C* q) { return q + ((128u - (smem_u32(q) & 127u)) & 127u) / sizeof(C); };
-  C* stg = ALIAS ? sh + 3 * LS : sh + xprod_stage_off(NX);
+  C* stg = ALIAS ? sh + 3 * LS : sh + xprod_stage_off(NX, (int)sizeof(C));
   if constexpr (JF) stg = align128(stg);
   C* const stg_out = ALIAS ? align128(sh) : stg;
   __shared__ uint64_t bar_al;
@@ -367,7 +379,10 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
     // tile in lies in 3..5 at 768 points, read by the first stage only)
     const XinvSh<C> xs = {stg, nxB, nx, NX};
     constexpr bool PP = XPROD_PP && Plan8<NT>::n == 3;
-    fft_sel<NT, +1, PPT, false, true, JF, false, PP>(NX, 3, twx + NX, sh, xs, L, sh + 3 * LS);
+    // FP64: the first stage reads rows 0 and 1 of the tile in side by side
+    // (conflict-free with the stride ls_x)
+    constexpr bool IL = XPROD_IL && PP && sizeof(C) == 16;
+    fft_sel<NT, +1, PPT, false, true, JF, false, PP, 0, IL>(NX, 3, twx + NX, sh, xs, L, sh + 3 * LS, LS);
   } else {
     const XinvSrc<C> xs = {Z + tile + yi0, cs, Ty, nx, NX};
     fft_sel<NT, +1, PPT, false, true, JF, false, false, XSH>(NX, 3, twx, sh, xs, L, sh, LS);
@@ -392,8 +407,15 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   const ProdSrc<LT, C> ps6 = {L, (T)ps.factor};
   fft_sel<NT, -1, PPT, true, true, JF, false, false, XSH>(NX, 6, JF ? twx + NX : twx, sh, ps6, L, sh, LS);
   __syncthreads();
-  // separate the two real transforms of each line, keep kx = 0..nx
-  if constexpr (ALIAS) {
+  // separate the two real transforms of each line, keep kx = 0..nx.  In
+  // FP64, with the tile out ([comp][ix][row]), item e is (row e & 1, mode
+  // e >> 1), so that a warp's stores are consecutive; the lines' stride
+  // (ls_x: 3 LS is half a bank row modulo a bank row) keeps the alternating
+  // reads of lines pl and pl + 3 on distinct banks too (384^2 x 256: 1.151
+  // -> 1.102 ms; in FP32 the same measured slower at 768 points, 7.66
+  // against 7.29 ms, and the items stay (mode, both rows)).
+  constexpr bool ALT = sizeof(C) == 16;
+  if constexpr (ALIAS && !ALT) {
     // the tile out overlays the lines: every thread reads its (at most two,
     // as 3 nxB <= NX <= 2 blockDim) entries first, then writes
     C zk[2][2], zm[2][2];
@@ -424,23 +446,58 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
         }
       }
     }
-  } else
-  for (int e = threadIdx.x; e < nxB * 3; e += blockDim.x) {
-    int pl = e / nxB, ix = e - pl * nxB;
+  } else if constexpr (ALIAS) {
+    // the tile out overlays the lines: every thread reads its (at most
+    // three, as 6 nxB <= 3 blockDim) entries first, then writes
+    C zk[3], zm[3];
 #pragma unroll
-    for (int yy = 0; yy < 2; ++yy) {
+    for (int k = 0; k < 3; ++k) {
+      const int e = threadIdx.x + k * blockDim.x;
+      if (e < nxB * 6) {
+        const int yy = e & 1, q = e >> 1, pl = q / nxB, ix = q - pl * nxB;
+        zk[k] = L(pl + 3 * yy, ix);
+        zm[k] = L(pl + 3 * yy, ix == 0 ? 0 : NX - ix);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int e = threadIdx.x + k * blockDim.x;
+      if (e < nxB * 6) {
+        const int yy = e & 1, q = e >> 1, pl = q / nxB, ix = q - pl * nxB;
+        const C Zk = zk[k], Zm = zm[k];
+        const T h = T(0.5);
+        stg_out[((2 * pl) * nxB + ix) * 2 + yy] = C{h * (Zk.x + Zm.x), h * (Zk.y - Zm.y)};
+        stg_out[((2 * pl + 1) * nxB + ix) * 2 + yy] = C{h * (Zk.y + Zm.y), h * (Zm.x - Zk.x)};
+      }
+    }
+  } else if constexpr (JF && ALT) {
+    for (int e = threadIdx.x; e < nxB * 6; e += blockDim.x) {
+      const int yy = e & 1, q = e >> 1, pl = q / nxB, ix = q - pl * nxB;
       const int ln = pl + 3 * yy;
       const C Zk = L(ln, ix), Zm = L(ln, ix == 0 ? 0 : NX - ix);
       const T h = T(0.5);
-      const C X = C{h * (Zk.x + Zm.x), h * (Zk.y - Zm.y)};
-      const C Y = C{h * (Zk.y + Zm.y), h * (Zm.x - Zk.x)};
-      if constexpr (JF) {
-        stg[((2 * pl) * nxB + ix) * 2 + yy] = X;
-        stg[((2 * pl + 1) * nxB + ix) * 2 + yy] = Y;
-      } else {
-        size_t o = tile + (size_t)ix * Ty + yi0 + yy;
-        Pp[(size_t)(2 * pl) * cs + o] = X;
-        Pp[(size_t)(2 * pl + 1) * cs + o] = Y;
+      stg[((2 * pl) * nxB + ix) * 2 + yy] = C{h * (Zk.x + Zm.x), h * (Zk.y - Zm.y)};
+      stg[((2 * pl + 1) * nxB + ix) * 2 + yy] = C{h * (Zk.y + Zm.y), h * (Zm.x - Zk.x)};
+    }
+  } else {
+    for (int e = threadIdx.x; e < nxB * 3; e += blockDim.x) {
+      int pl = e / nxB, ix = e - pl * nxB;
+#pragma unroll
+      for (int yy = 0; yy < 2; ++yy) {
+        const int ln = pl + 3 * yy;
+        const C Zk = L(ln, ix), Zm = L(ln, ix == 0 ? 0 : NX - ix);
+        const T h = T(0.5);
+        const C X = C{h * (Zk.x + Zm.x), h * (Zk.y - Zm.y)};
+        const C Y = C{h * (Zk.y + Zm.y), h * (Zm.x - Zk.x)};
+        if constexpr (JF) {
+          stg[((2 * pl) * nxB + ix) * 2 + yy] = X;
+          stg[((2 * pl + 1) * nxB + ix) * 2 + yy] = Y;
+        } else {
+          size_t o = tile + (size_t)ix * Ty + yi0 + yy;
+          Pp[(size_t)(2 * pl) * cs + o] = X;
+          Pp[(size_t)(2 * pl + 1) * cs + o] = Y;
+        }
       }
     }
   }
