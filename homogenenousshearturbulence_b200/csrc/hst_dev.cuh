@@ -313,9 +313,6 @@ struct LineGeom {
 // buf: the line (right-hand side in, solution out), in LineGeom layout.
 // fac: per-lane factor scratch, (m-2) x 4 x P doubles.
 // Rows of the right-hand side of KIND_DY must already hold D1 src.
-#ifndef HST_BACK_PF
-#define HST_BACK_PF 0
-#endif
 template <int P, class DST = SlabDer>
 __device__ void group_solve(int sys, double lambda, double ni, double kk, double theta, const DST& DS,
                             const LineGeom& G, cxd* buf, double* fac, int s, unsigned gmask) {
@@ -482,31 +479,6 @@ __device__ void group_solve(int sys, double lambda, double ni, double kk, double
   sb[mi + 1] = xb2;
   // back substitution (penta_backward :467-482)
   cxd xk1 = xb1, xk2 = xb2;
-#if HST_BACK_PF
-  // the factors of the next two rows are loaded while this row's chain
-  // runs (the scratch may live in L2)
-  double f[3][4];
-#pragma unroll
-  for (int q = 0; q < 2; ++q)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) f[q][c] = mi - 1 - q >= 0 ? fac[((mi - 1 - q) * 4 + c) * P + s] : 0.0;
-  for (int i = mi - 1; i >= 0; --i) {
-#pragma unroll
-    for (int c = 0; c < 4; ++c) f[2][c] = i - 2 >= 0 ? fac[((i - 2) * 4 + c) * P + s] : 0.0;
-    const double U1 = f[0][0], U2 = f[0][1], B1 = f[0][2], B2 = f[0][3];
-    cxd xr = sb[i];
-    cxd xk = mkc(xr.x - B1 * yb1.x - B2 * yb2.x - U1 * xk1.x - U2 * xk2.x,
-                 xr.y - B1 * yb1.y - B2 * yb2.y - U1 * xk1.y - U2 * xk2.y);
-    sb[i] = xk;
-    xk2 = xk1;
-    xk1 = xk;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      f[0][c] = f[1][c];
-      f[1][c] = f[2][c];
-    }
-  }
-#else
   for (int i = mi - 1; i >= 0; --i) {
     double U1 = fac[(i * 4 + 0) * P + s], U2 = fac[(i * 4 + 1) * P + s];
     double B1 = fac[(i * 4 + 2) * P + s], B2 = fac[(i * 4 + 3) * P + s];
@@ -517,7 +489,6 @@ __device__ void group_solve(int sys, double lambda, double ni, double kk, double
     xk2 = xk1;
     xk1 = xk;
   }
-#endif
 }
 
 // ------------------------------------- the D0 system, factored once ----

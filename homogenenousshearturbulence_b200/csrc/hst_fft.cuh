@@ -207,27 +207,7 @@ __host__ __device__ inline int ls_lines(int N, int nl) {
 // JF also selects the staged twiddle table: tw points at this stage's
 // block [r - 1][kk] of W^(kk r N/(Ns R)), r = 1..R-1, kk = 0..Ns-1, so that
 // a warp's twiddle loads are contiguous.
-// IL (with JF): butterfly b < 2 nb of lines 0 and 1 interleaved (line b & 1,
-// index b >> 1), the rest index-fastest from line 2 on; the x kernel's first
-// inverse stage, whose two reads a point from the tile in then hit
-// consecutive words for the two lines.
-template <bool JF, bool IL>
-__device__ __forceinline__ void stage_lj(int b, int nb, int nl, int& l, int& j) {
-  if constexpr (JF && IL) {
-    if (b < 2 * nb) {
-      l = b & 1;
-      j = b >> 1;
-    } else {
-      l = 2 + (b - 2 * nb) / nb;
-      j = (b - 2 * nb) % nb;
-    }
-  } else {
-    l = JF ? b / nb : b % nl;
-    j = JF ? b % nb : b / nl;
-  }
-}
-template <int R, int S, int PPT, bool SYNC, typename LD, typename ST, bool JF = false, typename C = cxd,
-          bool IL = false>
+template <int R, int S, int PPT, bool SYNC, typename LD, typename ST, bool JF = false, typename C = cxd>
 __device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const C* __restrict__ tw, const LD& ld,
                                              const ST& st) {
   constexpr int MAXB = (PPT + R - 1) / R;
@@ -241,8 +221,7 @@ __device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const C* __r
     int b = threadIdx.x + k * blockDim.x;
     lj[k] = -1;
     if (b < total) {
-      int l, j;
-      stage_lj<JF, IL>(b, nb, nl, l, j);
+      int l = JF ? b / nb : b % nl, j = JF ? b % nb : b / nl;
       int kk = j % Ns;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
@@ -262,8 +241,7 @@ __device__ __forceinline__ void fft_stage_io(int N, int nl, int Ns, const C* __r
 #pragma unroll
   for (int k = 0; k < MAXB; ++k) {
     if (lj[k] >= 0) {
-      int l, j;
-      stage_lj<JF, IL>(lj[k], nb, nl, l, j);
+      int l = JF ? lj[k] / nb : lj[k] % nl, j = JF ? lj[k] % nb : lj[k] / nl;
       int kk = j % Ns;
       int base = (j / Ns) * Ns * R + kk;
 #pragma unroll
@@ -350,9 +328,8 @@ template <> struct Plan8<768> { static constexpr int n = 3, r0 = 8, r1 = 8, r2 =
 // and dst not those at sh2.
 // XSH > 0: the caller's padded layout, one pad in 2^XSH at line stride lsx;
 // with JF, lsx > 0 is the stride of the padded lines (at least ls_padded).
-// IL: the first stage maps lines 0 and 1 interleaved (stage_lj).
-template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF, bool PZ, bool PP, int XSH, bool IL,
-          typename LD, typename ST, typename C>
+template <int N, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF, bool PZ, bool PP, int XSH, typename LD,
+          typename ST, typename C>
 __device__ __forceinline__ void fft_fixed(int nl, const C* __restrict__ tw, C* sh, const LD& src, const ST& dst,
                                           C* sh2, int lsx) {
   using PL = std::conditional_t<(PPT <= 8), Plan8<N>, Plan<N>>;
@@ -371,7 +348,7 @@ __device__ __forceinline__ void fft_fixed(int nl, const C* __restrict__ tw, C* s
   } else {
     // staged table (JF): stage 2's block first, then stage 3's
     const C* tw3 = JF ? tw + (PL::r1 - 1) * PL::r0 : tw;
-    fft_stage_io<PL::r0, S, PPT, SRC_SH, LD, LT, JF, C, IL>(N, nl, 1, tw, src, L);
+    fft_stage_io<PL::r0, S, PPT, SRC_SH, LD, LT, JF, C>(N, nl, 1, tw, src, L);
     __syncthreads();
     if constexpr (PP) {
       const LT L2 = {sh2, L.LS};
@@ -388,12 +365,12 @@ __device__ __forceinline__ void fft_fixed(int nl, const C* __restrict__ tw, C* s
 
 // NT > 0: the compile-time plan of length NT; NT = 0: the runtime plan of N.
 template <int NT, int S, int PPT, bool SRC_SH, bool DST_SH, bool JF = false, bool PZ = false, bool PP = false,
-          int XSH = 0, bool IL = false, typename LD, typename ST, typename C>
+          int XSH = 0, typename LD, typename ST, typename C>
 __device__ __forceinline__ void fft_sel(int N, int nl, const C* __restrict__ tw, C* sh, const LD& src,
                                         const ST& dst, C* sh2 = nullptr, int lsx = 0) {
-  static_assert(!(PZ || PP || XSH > 0 || IL) || NT > 0, "PZ, PP, XSH and IL need a compile-time plan");
+  static_assert(!(PZ || PP || XSH > 0) || NT > 0, "PZ, PP and XSH need a compile-time plan");
   if constexpr (NT > 0) {
-    fft_fixed<NT, S, PPT, SRC_SH, DST_SH, JF, PZ, PP, XSH, IL>(nl, tw, sh, src, dst, sh2, lsx);
+    fft_fixed<NT, S, PPT, SRC_SH, DST_SH, JF, PZ, PP, XSH>(nl, tw, sh, src, dst, sh2, lsx);
   } else {
     fft_global<S, PPT, SRC_SH, DST_SH>(N, nl, tw, sh, src, dst);
   }

@@ -268,9 +268,6 @@ struct ProdSrc {
 #ifndef XPAD1536
 #define XPAD1536 1
 #endif
-#ifndef XPROD_IL
-#define XPROD_IL 0
-#endif
 // line stride of the padded 1536-point x lines: 1728 + 3 (FP64) or + 11
 // (FP32), the strides that a CPU count of the plan's shared accesses ranks
 // best for three and six lines side by side
@@ -379,10 +376,7 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
     // tile in lies in 3..5 at 768 points, read by the first stage only)
     const XinvSh<C> xs = {stg, nxB, nx, NX};
     constexpr bool PP = XPROD_PP && Plan8<NT>::n == 3;
-    // FP64: the first stage reads rows 0 and 1 of the tile in side by side
-    // (conflict-free with the stride ls_x)
-    constexpr bool IL = XPROD_IL && PP && sizeof(C) == 16;
-    fft_sel<NT, +1, PPT, false, true, JF, false, PP, 0, IL>(NX, 3, twx + NX, sh, xs, L, sh + 3 * LS, LS);
+    fft_sel<NT, +1, PPT, false, true, JF, false, PP>(NX, 3, twx + NX, sh, xs, L, sh + 3 * LS, LS);
   } else {
     const XinvSrc<C> xs = {Z + tile + yi0, cs, Ty, nx, NX};
     fft_sel<NT, +1, PPT, false, true, JF, false, false, XSH>(NX, 3, twx, sh, xs, L, sh, LS);
