@@ -507,161 +507,6 @@ __global__ void __launch_bounds__(xprod_threads(NT, PPT), xprod_min_blocks(NT, P
   }
 }
 
-// The 768-point x kernel on a persistent grid of two blocks an SM: a block
-// walks the tiles t, t + gridDim.x, ... (t: pair of y rows fastest, then z
-// point, then member, the order of k_xprod's grid), and the tile in of its
-// next tile lands by TMA in a buffer of its own while the current one is
-// transformed (the buffer is read only by the first inverse stage; the load
-// is issued once every thread is past it).  The rest is k_xprod's ALIAS path.
-#ifndef XPROD_PERS
-#define XPROD_PERS 0
-#endif
-template <typename C>
-__host__ __device__ inline size_t xprod_pers_smem(int NX, int nxB) {
-  return ((size_t)6 * ls_x(NX, (int)sizeof(C)) + 6 * (size_t)nxB) * sizeof(C) + 256;
-}
-template <typename C>
-__global__ void __launch_bounds__(576, 2)
-    k_xprod_pers(Geometry g, const C* __restrict__ twx, const double* __restrict__ dyl, PhysScalars ps, int want_cfl,
-                 unsigned long long* __restrict__ cflmax, const __grid_constant__ CUtensorMap tmZ,
-                 const __grid_constant__ CUtensorMap tmP, int* __restrict__ err) {
-  constexpr int NT = 768, PPT = 8;
-  typedef typename RealOf<C>::T T;
-  extern __shared__ double2 sh_d[];
-  C* sh = reinterpret_cast<C*>(sh_d);
-  using LT = ShLinesPT<C>;
-  const int NX = 2 * g.nxd, nx = g.nx, nxB = g.nxB, NZ = g.nzd, Ty = g.Ty;
-  const int LS = ls_x(NX, (int)sizeof(C));
-  const LT L = {sh, LS};
-  auto align128 = [](C* q) { return q + ((128u - (smem_u32(q) & 127u)) & 127u) / sizeof(C); };
-  C* const pb = align128(sh + 6 * LS);  // the tile in of the next tile
-  C* const stg_out = align128(sh);
-  __shared__ uint64_t bar;
-  __shared__ int tile_ok;
-  const int npair = g.ny / 2;
-  const int ntiles = npair * NZ * g.nmem;
-  const unsigned tx = 3u * nxB * 2u * (unsigned)sizeof(C);
-  auto issue = [&](int t) {
-    const int q = t / npair, y0 = 2 * (t - q * npair), kz = q % NZ, mem = q / NZ;
-    const int yt = y0 / Ty, yi0 = y0 - yt * Ty;
-    mbar_arrive_expect_tx(&bar, tx);
-    tma_load_4d(pb, &tmZ, 2 * yi0, 0, yt * NZ + kz, 3 * mem, &bar);
-  };
-  if ((smem_u32(pb) & 127u) != 0 || (smem_u32(stg_out) & 127u) != 0) {  // never taken: aligned above
-    if (threadIdx.x == 0) atomicExch(err, 1);
-    return;
-  }
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    fence_mbar_init();
-    if ((int)blockIdx.x < ntiles) issue(blockIdx.x);
-  }
-  __syncthreads();
-  int it = 0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
-    const int q = t / npair, y0 = 2 * (t - q * npair), kz = q % NZ, mem = q / NZ;
-    const int yt = y0 / Ty, yi0 = y0 - yt * Ty;
-    if (threadIdx.x == 0) {
-      const bool ok = mbar_wait_bounded(&bar, it & 1, XPROD_WAIT_LIMIT);
-      if (!ok) {
-        // record the failure and give the copy a second bounded wait
-        // before the block (and its shared memory) goes away
-        atomicExch(err, 1);
-        mbar_wait_bounded(&bar, it & 1, XPROD_WAIT_LIMIT);
-      }
-      tile_ok = ok;
-    }
-    // (this barrier also orders the lines' writes below after the previous
-    // tile's tensor store has read them: thread 0 waited for it)
-    __syncthreads();
-    if (!tile_ok) break;
-    {
-      const XinvSh<C> xs = {pb, nxB, nx, NX};
-      fft_sel<NT, +1, PPT, false, true, true, false, true>(NX, 3, twx + NX, sh, xs, L, sh + 3 * LS, LS);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) {
-      fence_proxy_async();
-      issue(t + gridDim.x);
-    }
-    if (want_cfl) {
-      double cm = 0.0;
-      const double rdy0 = dyl[y0], rdy1 = dyl[y0 + 1];
-      for (int x = threadIdx.x; x < NX; x += blockDim.x) {
-        const C a0 = L(0, x), a1 = L(1, x), b = L(2, x);
-        double c0 = fabs((double)a0.x) / ps.dx + fabs((double)a0.y) / rdy0 + fabs((double)b.x) / ps.dz;
-        double c1 = fabs((double)a1.x) / ps.dx + fabs((double)a1.y) / rdy1 + fabs((double)b.y) / ps.dz;
-        cm = nan_max(cm, nan_max(c0, c1));
-      }
-      for (int o = 16; o > 0; o >>= 1) cm = nan_max(cm, __shfl_xor_sync(0xffffffffu, cm, o));
-      if ((threadIdx.x & 31) == 0) atomicMax(cflmax, (unsigned long long)__double_as_longlong(cm));
-    }
-    const ProdSrc<LT, C> ps6 = {L, (T)ps.factor};
-    fft_sel<NT, -1, PPT, true, true, true, false, false>(NX, 6, twx + NX, sh, ps6, L, sh, LS);
-    __syncthreads();
-    if constexpr (sizeof(C) == 16) {
-      C zk[3], zm[3];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const int e = threadIdx.x + k * blockDim.x;
-        if (e < nxB * 6) {
-          const int yy = e & 1, qq = e >> 1, pl = qq / nxB, ix = qq - pl * nxB;
-          zk[k] = L(pl + 3 * yy, ix);
-          zm[k] = L(pl + 3 * yy, ix == 0 ? 0 : NX - ix);
-        }
-      }
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const int e = threadIdx.x + k * blockDim.x;
-        if (e < nxB * 6) {
-          const int yy = e & 1, qq = e >> 1, pl = qq / nxB, ix = qq - pl * nxB;
-          const C Zk = zk[k], Zm = zm[k];
-          const T h = T(0.5);
-          stg_out[((2 * pl) * nxB + ix) * 2 + yy] = C{h * (Zk.x + Zm.x), h * (Zk.y - Zm.y)};
-          stg_out[((2 * pl + 1) * nxB + ix) * 2 + yy] = C{h * (Zk.y + Zm.y), h * (Zm.x - Zk.x)};
-        }
-      }
-    } else {
-      C zk[2][2], zm[2][2];
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int e = threadIdx.x + k * blockDim.x;
-        if (e < nxB * 3) {
-          const int pl = e / nxB, ix = e - pl * nxB;
-#pragma unroll
-          for (int yy = 0; yy < 2; ++yy) {
-            zk[k][yy] = L(pl + 3 * yy, ix);
-            zm[k][yy] = L(pl + 3 * yy, ix == 0 ? 0 : NX - ix);
-          }
-        }
-      }
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int e = threadIdx.x + k * blockDim.x;
-        if (e < nxB * 3) {
-          const int pl = e / nxB, ix = e - pl * nxB;
-#pragma unroll
-          for (int yy = 0; yy < 2; ++yy) {
-            const C Zk = zk[k][yy], Zm = zm[k][yy];
-            const T h = T(0.5);
-            stg_out[((2 * pl) * nxB + ix) * 2 + yy] = C{h * (Zk.x + Zm.x), h * (Zk.y - Zm.y)};
-            stg_out[((2 * pl + 1) * nxB + ix) * 2 + yy] = C{h * (Zk.y + Zm.y), h * (Zm.x - Zk.x)};
-          }
-        }
-      }
-    }
-    fence_proxy_async();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      tma_store_4d(&tmP, 2 * yi0, 0, yt * NZ + kz, 6 * mem, stg_out);
-      bulk_commit();
-      bulk_wait_read_all();
-    }
-  }
-}
-
 // --------------------------------------- the reference-layout transforms ----
 // FFT, IFT, RFT and HFT (src/hst_fft.f90:181-237) on the buffers of the
 // per-piece path, which hold the reference's layouts: VVdz(nzd, nx+1,
@@ -976,22 +821,6 @@ static cudaError_t launch_xprod_main(const Geometry& g, const DeviceState& d, co
   const int pts = 6 * NX;
   if (xprod_uses_maps(g) != d.maps) return cudaErrorInvalidValue;
   const dim3 grid(g.ny / 2, g.nzd * g.nmem);
-  if (XPROD_PERS && NX == 768 && g.pptx == 8 && xprod_uses_maps(g)) {
-    const int ntiles = g.ny / 2 * g.nzd * g.nmem;
-    const int nb = std::min(ntiles, 2 * (d.nsm > 0 ? d.nsm : 148));
-    if (g.mp) {
-      typedef float2 C;
-      big_smem(d, k_xprod_pers<C>);
-      k_xprod_pers<C><<<nb, 576, xprod_pers_smem<C>(NX, g.nxB), st>>>(g, d.twxf, d.dyl, ph, want_cfl, d.cfl, d.tmZ,
-                                                                       d.tmPp, d.err);
-    } else {
-      typedef double2 C;
-      big_smem(d, k_xprod_pers<C>);
-      k_xprod_pers<C><<<nb, 576, xprod_pers_smem<C>(NX, g.nxB), st>>>(g, d.twx, d.dyl, ph, want_cfl, d.cfl, d.tmZ,
-                                                                       d.tmPp, d.err);
-    }
-    return cudaGetLastError();
-  }
   if (g.mp) {
     typedef float2 C;
     const size_t lines = (size_t)6 * (NX == 1536 && XPAD1536 ? xls_1536(8) : NX + 1) * sizeof(C);
