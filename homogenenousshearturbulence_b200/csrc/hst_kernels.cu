@@ -350,78 +350,6 @@ __device__ __forceinline__ void slab_stencil(int n, const DST& DS, cxd* sb, int 
 }
 
 
-#ifndef HST_SHIFT_FUSE
-#define HST_SHIFT_FUSE 0  // 1: the exact_shift node phases applied inside the D0 stencil pass
-#endif
-// slab_stencil (n = 0) of the line times the node phases e_k of its rows
-// (row s m + k of lane s: e_0 = e0, e_(k+1) = e_k estep on a uniform grid,
-// else exp(-i gx y)), the phases taken as the window reads each row instead
-// of in a pass of their own: the same products in the same order, one
-// shared-memory pass over the line fewer.
-template <int P, class DST>
-__device__ __forceinline__ void slab_stencil_phased(const DST& DS, cxd* sb, int m, int s, cxd ph, unsigned gmask,
-                                                    cxd e0, cxd estep, bool yuni, double gx, const double* ys) {
-  auto phase_at = [&](int k, cxd ek) { return yuni || k == 0 ? ek : cexpi(-gx * ys[k]); };
-  // the phases of rows m-2, m-1 (the rows the lane below needs), by the
-  // same recurrence as the main loop
-  cxd em2 = e0, em1 = e0;
-  {
-    cxd e = e0;
-    for (int k = 0; k < m; ++k) {
-      const cxd ek = phase_at(k, e);
-      if (k == m - 2) em2 = ek;
-      if (k == m - 1) em1 = ek;
-      e = cmul(ek, estep);
-    }
-  }
-  cxd e = e0;
-  const cxd e_0 = phase_at(0, e);
-  e = cmul(e_0, estep);
-  const cxd e_1 = phase_at(1, e);
-  e = cmul(e_1, estep);
-  const cxd e_2 = phase_at(2, e);
-  e = cmul(e_2, estep);  // the recurrence's value for row 3
-  const cxd f0 = cmul(sb[0], e_0), f1 = cmul(sb[1], e_1), l0 = cmul(sb[m - 2], em2), l1 = cmul(sb[m - 1], em1);
-  const int up = (s + 1) & (P - 1), dn = (s - 1) & (P - 1);
-  cxd a0 = shfl_c(gmask, f0, up, P), a1 = shfl_c(gmask, f1, up, P);
-  cxd b0 = shfl_c(gmask, l0, dn, P), b1 = shfl_c(gmask, l1, dn, P);
-  if (s == P - 1) {
-    a0 = cmul(a0, ph);
-    a1 = cmul(a1, ph);
-  }
-  if (s == 0) {
-    b0 = cmul(b0, cconj(ph));
-    b1 = cmul(b1, cconj(ph));
-  }
-  cxd w0 = b0, w1 = b1, w2 = f0, w3 = f1, w4 = cmul(sb[2], e_2);
-#pragma unroll 2
-  for (int i = 0; i < m; ++i) {
-    const double c0 = DS(s, i, 0, 0), c1 = DS(s, i, 0, 1), c2 = DS(s, i, 0, 2), c3 = DS(s, i, 0, 3),
-                 c4 = DS(s, i, 0, 4);
-    cxd acc = mkc(0, 0);
-    acc = mkc(acc.x + c0 * w0.x, acc.y + c0 * w0.y);
-    acc = mkc(acc.x + c1 * w1.x, acc.y + c1 * w1.y);
-    acc = mkc(acc.x + c2 * w2.x, acc.y + c2 * w2.y);
-    acc = mkc(acc.x + c3 * w3.x, acc.y + c3 * w3.y);
-    acc = mkc(acc.x + c4 * w4.x, acc.y + c4 * w4.y);
-    const int nx = i + 3;
-    cxd nxt;
-    if (nx < m) {
-      const cxd en = phase_at(nx, e);
-      nxt = cmul(sb[nx], en);
-      e = cmul(en, estep);
-    } else {
-      nxt = nx == m ? a0 : a1;
-    }
-    sb[i] = acc;
-    w0 = w1;
-    w1 = w2;
-    w2 = w3;
-    w3 = w4;
-    w4 = nxt;
-  }
-}
-
 // The solve stage on one column, for MODE COL_SOLVE (and COL_SHIFT: the
 // exact_shift shift alone) with the lines and every intermediate in shared
 // memory: no scratch column of V is written and read back.
@@ -482,14 +410,6 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, i
         group_solve_d0<P, 1, SHT>(th0, SHT ? d0s : a.d0tab, G, bufs, s, gmask);
       }
       __syncwarp(gmask);
-#if HST_SHIFT_FUSE
-      // the node phases applied as the D0 stencil reads the rows
-      if constexpr (SHT)
-        slab_stencil_phased<P>(SlabDerT<true>{der0s, m, P}, sX, m, s, phs, gmask, e0, estep, sc.yuni, gx,
-                               a.y + s * m + 2);
-      else
-        slab_stencil_phased<P>(DS, sX, m, s, phs, gmask, e0, estep, sc.yuni, gx, a.y + s * m + 2);
-#else
       cxd e = e0;
       for (int i = 0; i < m; ++i) {
         if (!sc.yuni && i > 0) e = cexpi(-gx * a.y[s * m + i + 2]);
@@ -501,7 +421,6 @@ __device__ __forceinline__ void column_solve_body(const ColumnArgs& a, int cg, i
         slab_stencil<P>(0, SlabDerT<true>{der0s, m, P}, sX, m, s, phs, gmask);
       else
         slab_stencil<P>(0, DS, sX, m, s, phs, gmask);
-#endif
       __syncwarp(gmask);
       if (q < 2 || SHIFT_ONLY) {
         double2* dst = q == 0 ? a.O1 : (q == 1 ? a.O2 : (q == 2 ? a.R1 : a.R2));
